@@ -1,0 +1,100 @@
+/*
+ * pfsoft_b200 -- C ABI of the B200 SO(3) Fourier transform engine (DSOFT / iDSOFT).
+ *
+ * Drop-in boundary for PFSOFTlib's hot path. Every entry point takes plain pointers and
+ * sizes; `stream` is a cudaStream_t passed as void* (NULL = the legacy default stream).
+ * All functions return a pfsoft_status; pfsoft_last_error() gives the detail of the last
+ * failure on the calling thread. Nothing here exits the process: where the reference prints a
+ * warning and returns (src/fn_dsoft.cpp:82-94, src/fn_idsoft.cpp:78-90 via
+ * cmake_aux/compiler_config.hpp.in:112-120) these functions return PFSOFT_EINVAL.
+ *
+ * Layouts (N = 2B, complex values as interleaved {re, im} doubles):
+ *   grid    N*N*N complex; element (row, col, lay) at (lay*N + col)*N + row, the layout of the
+ *           reference's grid3D<complex<double>> (include/PFSOFTlib_headers/grid3D_cx.hpp:293-303).
+ *   coeffs  B(4B^2-1)/3 complex; degree l starts at l(4l^2-1)/3 and holds a column-major
+ *           (2l+1)x(2l+1) block, row index M, column index M', a negative order M stored at
+ *           2l+1+M -- the storage of DSOFTFourierCoefficients
+ *           (src/dsoft_fourier_coefficients.cpp:48-57, :80-89), packed contiguously.
+ *
+ * First use of a bandwidth on a device builds its constant tables (one cudaMalloc and one
+ * small kernel, then a stream synchronisation); make that first call before any stream
+ * capture. Later calls for the same bandwidth allocate nothing.
+ */
+#ifndef PFSOFT_B200_H
+#define PFSOFT_B200_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum pfsoft_status {
+    PFSOFT_OK = 0,
+    PFSOFT_EINVAL = 1,   /* bad argument (size, pointer, bandwidth mismatch) */
+    PFSOFT_ENOMEM = 2,   /* device or pinned allocation failed / budget exceeded */
+    PFSOFT_ETIMEOUT = 3, /* a bounded wait ran out */
+    PFSOFT_ECUDA = 4,    /* a CUDA runtime call failed */
+    PFSOFT_EBUSY = 5     /* a resource is in use (serving queue full) */
+} pfsoft_status;
+
+const char* pfsoft_status_string(int status);
+/* Detail of the most recent failure on this thread ("" if none). */
+const char* pfsoft_last_error(void);
+/* Library version as MAJOR*10000 + MINOR*100 + PATCH. */
+int pfsoft_version(void);
+
+/* Sizes. */
+size_t pfsoft_coef_count(int B);            /* B(4B^2-1)/3 complex values */
+size_t pfsoft_grid_bytes(int B);            /* (2B)^3 * 16 */
+size_t pfsoft_workspace_bytes(int B);       /* device scratch for one transform */
+
+/* ---- Forward / inverse transforms on device-resident data (stream ordered) -------------
+ * pfsoft_cuda_dsoft replaces pfsoft::FourierTransforms::DSOFT
+ *   (include/PFSOFTlib_headers/fn_fourier_transforms.hpp:75, src/fn_dsoft.cpp:76).
+ *   d_grid is not modified (the reference takes the grid by value). d_coeffs receives all
+ *   B(4B^2-1)/3 coefficients. d_workspace: pfsoft_workspace_bytes(B) bytes of device memory,
+ *   or NULL to use a library-owned buffer (allocated on first use, then reused; calls that
+ *   share it are serialised on `stream` order only, so do not pass NULL from two streams).
+ * pfsoft_cuda_idsoft replaces pfsoft::FourierTransforms::IDSOFT
+ *   (fn_fourier_transforms.hpp:78, src/fn_idsoft.cpp:72). Every grid value is written; the
+ *   Nyquist bins (row or col order == B), which the reference leaves as it found them, are
+ *   synthesised from zero, i.e. the result the reference gives on a fresh grid.
+ */
+int pfsoft_cuda_dsoft(const double* d_grid, int B, double* d_coeffs, void* d_workspace,
+                      size_t workspace_bytes, void* stream);
+int pfsoft_cuda_idsoft(const double* d_coeffs, int B, double* d_grid, void* d_workspace,
+                       size_t workspace_bytes, void* stream);
+
+/* ---- Host-resident drop-in (synchronous) ---------------------------------------------------
+ * The same transforms on host buffers: copy in, transform, copy out, wait. Pinned host
+ * buffers (cudaHostAlloc) make the copies asynchronous DMA; pageable ones work too.
+ * Calls on one device are serialised by the library (its staging buffers are shared). */
+int pfsoft_dsoft_host(const double* h_grid, int B, double* h_coeffs);
+int pfsoft_idsoft_host(const double* h_coeffs, int B, double* h_grid);
+
+/* ---- FFT boundary ------------------------------------------------------------------------
+ * Replace the reference's internal C ABI uzl_fftw_layer_wise_DFT2_grid3D /
+ * uzl_fftw_layer_wise_IDFT2_grid3D (include/PFSOFTlib_headers/fftw_wrapper.hpp:31-32,
+ * src/fftw_wrapper.cpp:47-173): an in-place 2D DFT of each of `lays` layers of cols x rows
+ * complex values (rows contiguous), exp(-i..) for DFT2 and exp(+i..) for IDFT2, every value
+ * multiplied by `scale` (1.0 = unnormalised, as FFTW). `threads` of the reference has no
+ * counterpart. */
+int pfsoft_cuda_layer_wise_dft2(int cols, int rows, int lays, double* d_arr, double scale, void* stream);
+int pfsoft_cuda_layer_wise_idft2(int cols, int rows, int lays, double* d_arr, double scale, void* stream);
+
+/* ---- Discrete Wigner transform helpers ---------------------------------------------------
+ * pfsoft_cuda_quadrature_weights replaces DWT::quadrature_weights
+ *   (include/PFSOFTlib_headers/fn_dwt.hpp:64): d_w receives w_B(j), j < 2B.
+ * pfsoft_cuda_wigner_d_matrix replaces DWT::wigner_d_matrix / weighted_wigner_d_matrix
+ *   (fn_dwt.hpp:239, :107): rows l = J..B-1 (J = max(|M|,|M'|)) by 2B columns, written
+ *   row-major d_out[(l-J)*2B + k] (the reference's matrix is column-major; transpose on the
+ *   caller side if needed). weighted != 0 multiplies column k by w_B(k). */
+int pfsoft_cuda_quadrature_weights(int B, double* d_w, void* stream);
+int pfsoft_cuda_wigner_d_matrix(int B, int M, int Mp, int weighted, double* d_out, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* PFSOFT_B200_H */

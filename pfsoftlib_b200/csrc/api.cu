@@ -1,0 +1,513 @@
+// C ABI of the engine (include/pfsoft_b200.h): argument checks, per-device caches of the
+// bandwidth tables and scratch buffers, and the stream-ordered launch sequences.
+//
+//   forward  (src/fn_dsoft.cpp:76)  grid --F1--> X --F2--> X --DWT--> coeffs
+//            F1: DFT over gamma (rows) of every (beta, alpha) row, written beta-innermost
+//            F2: DFT over alpha of every (gamma-bin, beta) column, in place
+//   inverse  (src/fn_idsoft.cpp:72) coeffs --iDWT--> X --I2--> X --I1--> grid (x 1/N^2)
+
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/pfsoft_b200.h"
+#include "common.cuh"
+#include "dwt.cuh"
+#include "fft.cuh"
+
+using namespace pfsoft_dev;
+
+namespace {
+
+thread_local std::string g_last_error;
+
+int fail(int status, const std::string& msg)
+{
+    g_last_error = msg;
+    return status;
+}
+
+int cuda_fail(cudaError_t e, const char* what)
+{
+    return fail(PFSOFT_ECUDA, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+#define PF_CUDA(call)                                   \
+    do {                                                \
+        cudaError_t e_ = (call);                        \
+        if (e_ != cudaSuccess) return cuda_fail(e_, #call); \
+    } while (0)
+
+constexpr int kMaxBandwidth = 512;
+constexpr int kFftKB = 8;   // vectors per FFT tile: 8 complex128 = 128 contiguous bytes
+
+struct DeviceState {
+    std::mutex mu;
+    std::map<int, BandTables> tables;
+    void* ws = nullptr;          // library-owned workspace (NULL-workspace calls)
+    size_t ws_bytes = 0;
+    // host-staged calls
+    std::mutex host_mu;
+    void* h_grid = nullptr;
+    void* h_coef = nullptr;
+    void* h_ws = nullptr;
+    size_t h_grid_bytes = 0, h_coef_bytes = 0, h_ws_bytes = 0;
+    cudaStream_t h_stream = nullptr;
+};
+
+std::mutex g_devices_mu;
+std::map<int, DeviceState*> g_devices;
+
+DeviceState* device_state(int dev)
+{
+    std::lock_guard<std::mutex> lk(g_devices_mu);
+    auto it = g_devices.find(dev);
+    if (it != g_devices.end()) return it->second;
+    DeviceState* s = new DeviceState();   // lives until process exit
+    g_devices[dev] = s;
+    return s;
+}
+
+bool valid_bandwidth(int B) { return B >= 1 && B <= kMaxBandwidth; }
+
+size_t grid_elems(int B)
+{
+    const size_t N = 2 * (size_t)B;
+    return N * N * N;
+}
+
+// Tables for bandwidth B on the current device; built on first use.
+int get_tables(int B, cudaStream_t stream, BandTables* out)
+{
+    int dev = 0;
+    PF_CUDA(cudaGetDevice(&dev));
+    DeviceState* st = device_state(dev);
+    std::lock_guard<std::mutex> lk(st->mu);
+    auto it = st->tables.find(B);
+    if (it != st->tables.end()) {
+        *out = it->second;
+        return PFSOFT_OK;
+    }
+    void* mem = nullptr;
+    cudaError_t e = cudaMalloc(&mem, tables_bytes(B));
+    if (e != cudaSuccess) return fail(PFSOFT_ENOMEM, std::string("table allocation: ") + cudaGetErrorString(e));
+    BandTables t;
+    e = tables_build(B, mem, &t, stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
+    if (e != cudaSuccess) {
+        cudaFree(mem);
+        return cuda_fail(e, "tables_build");
+    }
+    st->tables[B] = t;
+    *out = t;
+    return PFSOFT_OK;
+}
+
+// Library-owned workspace of at least `bytes` on the current device.
+int get_workspace(size_t bytes, void** ws)
+{
+    int dev = 0;
+    PF_CUDA(cudaGetDevice(&dev));
+    DeviceState* st = device_state(dev);
+    std::lock_guard<std::mutex> lk(st->mu);
+    if (st->ws_bytes < bytes) {
+        if (st->ws) {
+            cudaDeviceSynchronize();
+            cudaFree(st->ws);
+            st->ws = nullptr;
+            st->ws_bytes = 0;
+        }
+        cudaError_t e = cudaMalloc(&st->ws, bytes);
+        if (e != cudaSuccess) return fail(PFSOFT_ENOMEM, std::string("workspace allocation: ") + cudaGetErrorString(e));
+        st->ws_bytes = bytes;
+    }
+    *ws = st->ws;
+    return PFSOFT_OK;
+}
+
+FftPassArgs pass_args(int n, int nvec, const BandTables& t, FftStrides src, FftStrides dst, double scale)
+{
+    FftPassArgs a;
+    memset(&a, 0, sizeof(a));
+    a.n = n;
+    a.nvec = nvec;
+    a.kb = kFftKB;
+    a.nstages = fft_plan_radices(n, a.radix, a.ns);
+    a.src = src;
+    a.dst = dst;
+    a.scale = scale;
+    a.twiddle = t.twiddle;
+    return a;
+}
+
+DwtArgs dwt_args(const BandTables& t)
+{
+    DwtArgs a;
+    a.B = t.B;
+    a.N = t.N;
+    a.cosb = t.cosb;
+    a.sinh = t.sinh;
+    a.cosh = t.cosh;
+    a.w = t.w;
+    a.normf = t.normf;
+    a.team_warps = dwt_team_warps(t.N);
+    return a;
+}
+
+int dwt_blocks(int B, int team_warps)
+{
+    const int teams_per_cta = 4 / team_warps;
+    const int need = (num_classes(B) + teams_per_cta - 1) / teams_per_cta;
+    int dev = 0, sms = 148;
+    if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    const int cap = sms * 8;
+    return need < cap ? need : cap;
+}
+
+int check_transform_args(const void* a, const void* b, int B, void*& ws, size_t ws_bytes)
+{
+    if (!valid_bandwidth(B)) return fail(PFSOFT_EINVAL, "bandwidth must be in [1, 512]");
+    if (!a || !b) return fail(PFSOFT_EINVAL, "null data pointer");
+    const size_t need = grid_elems(B) * sizeof(double2);
+    if (ws) {
+        if (ws_bytes < need) return fail(PFSOFT_EINVAL, "workspace smaller than pfsoft_workspace_bytes(B)");
+        if ((reinterpret_cast<uintptr_t>(ws) & 15) != 0) return fail(PFSOFT_EINVAL, "workspace not 16-byte aligned");
+        return PFSOFT_OK;
+    }
+    return get_workspace(need, &ws);
+}
+
+int run_dsoft(const double* d_grid, int B, double* d_coeffs, void* ws, cudaStream_t s)
+{
+    BandTables t;
+    int rc = get_tables(B, s, &t);
+    if (rc) return rc;
+    const int N = 2 * B;
+    const long long n = N, n2 = n * n;
+    const double2* G = reinterpret_cast<const double2*>(d_grid);
+    double2* X = static_cast<double2*>(ws);
+    // F1: vectors = layers k, tile = column c, elements = rows r; G[k][c][r] -> X[r][c][k]
+    FftPassArgs f1 = pass_args(N, N, t, FftStrides{n2, n, 1}, FftStrides{1, n, n2}, 1.0);
+    // F2: vectors = layers k, tile = gamma bin r, elements = column c; in place on X
+    FftPassArgs f2 = pass_args(N, N, t, FftStrides{1, n2, n}, FftStrides{1, n2, n}, 1.0);
+    if (f1.nstages == 0) return fail(PFSOFT_EINVAL, "FFT length cannot be planned");
+    PF_CUDA(fft_pass_launch(G, X, f1, N, -1, s));
+    PF_CUDA(fft_pass_launch(X, X, f2, N, -1, s));
+    DwtArgs a = dwt_args(t);
+    PF_CUDA(dwt_forward_launch(X, reinterpret_cast<double2*>(d_coeffs), a, dwt_blocks(B, a.team_warps), s));
+    return PFSOFT_OK;
+}
+
+int run_idsoft(const double* d_coeffs, int B, double* d_grid, void* ws, cudaStream_t s)
+{
+    BandTables t;
+    int rc = get_tables(B, s, &t);
+    if (rc) return rc;
+    const int N = 2 * B;
+    const long long n = N, n2 = n * n;
+    double2* X = static_cast<double2*>(ws);
+    double2* G = reinterpret_cast<double2*>(d_grid);
+    PF_CUDA(zero_nyquist_launch(X, B, s));
+    DwtArgs a = dwt_args(t);
+    PF_CUDA(dwt_inverse_launch(reinterpret_cast<const double2*>(d_coeffs), X, a, dwt_blocks(B, a.team_warps), s));
+    // I2: inverse DFT over alpha, in place on X
+    FftPassArgs i2 = pass_args(N, N, t, FftStrides{1, n2, n}, FftStrides{1, n2, n}, 1.0);
+    // I1: inverse DFT over gamma, X[r][c][k] -> G[k][c][r], scaled by 1/(4B^2) (src/fn_idsoft.cpp:289)
+    FftPassArgs i1 = pass_args(N, N, t, FftStrides{1, n, n2}, FftStrides{n2, n, 1}, 1.0 / (4.0 * B * B));
+    if (i1.nstages == 0) return fail(PFSOFT_EINVAL, "FFT length cannot be planned");
+    PF_CUDA(fft_pass_launch(X, X, i2, N, +1, s));
+    PF_CUDA(fft_pass_launch(X, G, i1, N, +1, s));
+    return PFSOFT_OK;
+}
+
+// ---- small kernels for the DWT helper API ---------------------------------------------------
+
+__global__ void copy_weights_kernel(const double* w, double* out, int N)
+{
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < N; k += gridDim.x * blockDim.x) out[k] = w[k];
+}
+
+// One thread per beta column; the reference's seed cases for any signs of (M, Mp)
+// (fn_dwt.hpp:112-163) and its recurrence (:167-199).
+__global__ void wigner_matrix_kernel(int B, int M, int Mp, const double* w, const double* cosb, const double* sinh,
+                                     const double* cosh, double* out)
+{
+    const int N = 2 * B;
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= N) return;
+    const int aM = M < 0 ? -M : M, aMp = Mp < 0 ? -Mp : Mp;
+    const int J = aM > aMp ? aM : aMp, Jmin = aM < aMp ? aM : aMp;
+    double nf = sqrt((2.0 * J + 1.0) / 2.0);
+    for (int i = 0; i < J - Jmin; ++i) nf *= sqrt((2.0 * J - i) / (i + 1.0));
+    int cp, sp;
+    if (J == aM && M >= 0) { cp = J + Mp; sp = J - Mp; }
+    else if (J == aM)      { cp = J - Mp; sp = J + Mp; }
+    else if (Mp >= 0)      { cp = J + M;  sp = J - M;  }
+    else                   { cp = J - M;  sp = J + M;  }
+    const double scale_w = w ? w[k] : 1.0;
+    // extended-exponent seed (as in the DWT kernels)
+    int xe;
+    double ms = 1.0, mc = 1.0;
+    int es = 0, ec = 0;
+    {
+        double xm = frexp(sinh[k], &xe);
+        int p = sp;
+        while (p) {
+            if (p & 1) { int t2; ms = frexp(ms * xm, &t2); es += xe + t2; }
+            p >>= 1;
+            if (p) { int t2; xm = frexp(xm * xm, &t2); xe = 2 * xe + t2; }
+        }
+        xm = frexp(cosh[k], &xe);
+        p = cp;
+        while (p) {
+            if (p & 1) { int t2; mc = frexp(mc * xm, &t2); ec += xe + t2; }
+            p >>= 1;
+            if (p) { int t2; xm = frexp(xm * xm, &t2); xe = 2 * xe + t2; }
+        }
+    }
+    int ev;
+    const double v = frexp(nf * scale_w * ms * mc, &ev);
+    const int E = ev + es + ec;
+    int sc = 0;
+    double dcur;
+    if (E >= -900) {
+        dcur = -ldexp(v, E);
+    } else {
+        sc = (-900 - E + 599) / 600;
+        dcur = -ldexp(v, E + 600 * sc);
+    }
+    double dprev = 0.0;
+    const double cb = cosb[k];
+    for (int l = J; l < B; ++l) {
+        out[(size_t)(l - J) * N + k] = sc ? ldexp(dcur, -600 * sc) : dcur;
+        if (l + 1 >= B) break;
+        const double idx = (double)l;
+        const double nrm = sqrt((2.0 * idx + 3.0) / (2.0 * idx + 1.0));
+        const double nom = (idx + 1.0) * (2.0 * idx + 1.0);
+        const double den = 1.0 / sqrt(((idx + 1) * (idx + 1) - (double)M * M) * ((idx + 1) * (idx + 1) - (double)Mp * Mp));
+        const double f1 = nrm * nom * den;
+        double c1 = 0.0, f2 = 0.0;
+        if (l != 0) {
+            const double t1 = sqrt((2.0 * idx + 3.0) / (2.0 * idx - 1.0)) * (idx + 1.0) / idx;
+            const double t2 = sqrt((idx * idx - (double)M * M) * (idx * idx - (double)Mp * Mp));
+            c1 = -t1 * t2 * den;
+            f2 = -(double)M * Mp / (idx * (idx + 1.0));
+        }
+        const double nx = fma(c1, dprev, (dcur * f1) * (f2 + cb));
+        dprev = dcur;
+        dcur = nx;
+        if (sc && fabs(dcur) >= 0x1p300) {
+            dcur *= 0x1p-600;
+            dprev *= 0x1p-600;
+            --sc;
+        }
+    }
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* pfsoft_status_string(int status)
+{
+    switch (status) {
+        case PFSOFT_OK: return "ok";
+        case PFSOFT_EINVAL: return "invalid argument";
+        case PFSOFT_ENOMEM: return "out of memory";
+        case PFSOFT_ETIMEOUT: return "timed out";
+        case PFSOFT_ECUDA: return "CUDA error";
+        case PFSOFT_EBUSY: return "busy";
+        default: return "unknown status";
+    }
+}
+
+const char* pfsoft_last_error(void) { return g_last_error.c_str(); }
+
+int pfsoft_version(void) { return 100; }
+
+size_t pfsoft_coef_count(int B) { return B < 1 ? 0 : coef_offset(B); }
+
+size_t pfsoft_grid_bytes(int B) { return B < 1 ? 0 : grid_elems(B) * sizeof(double2); }
+
+size_t pfsoft_workspace_bytes(int B) { return B < 1 ? 0 : grid_elems(B) * sizeof(double2); }
+
+int pfsoft_cuda_dsoft(const double* d_grid, int B, double* d_coeffs, void* d_workspace, size_t workspace_bytes,
+                      void* stream)
+{
+    g_last_error.clear();
+    int rc = check_transform_args(d_grid, d_coeffs, B, d_workspace, workspace_bytes);
+    if (rc) return rc;
+    return run_dsoft(d_grid, B, d_coeffs, d_workspace, static_cast<cudaStream_t>(stream));
+}
+
+int pfsoft_cuda_idsoft(const double* d_coeffs, int B, double* d_grid, void* d_workspace, size_t workspace_bytes,
+                       void* stream)
+{
+    g_last_error.clear();
+    int rc = check_transform_args(d_coeffs, d_grid, B, d_workspace, workspace_bytes);
+    if (rc) return rc;
+    return run_idsoft(d_coeffs, B, d_grid, d_workspace, static_cast<cudaStream_t>(stream));
+}
+
+static int host_staged(int B, bool forward, const double* in, double* out)
+{
+    g_last_error.clear();
+    if (!valid_bandwidth(B)) return fail(PFSOFT_EINVAL, "bandwidth must be in [1, 512]");
+    if (!in || !out) return fail(PFSOFT_EINVAL, "null host pointer");
+    int dev = 0;
+    PF_CUDA(cudaGetDevice(&dev));
+    DeviceState* st = device_state(dev);
+    std::lock_guard<std::mutex> lk(st->host_mu);
+    const size_t gb = grid_elems(B) * sizeof(double2);
+    const size_t cb = coef_offset(B) * sizeof(double2);
+    if (!st->h_stream) PF_CUDA(cudaStreamCreateWithFlags(&st->h_stream, cudaStreamNonBlocking));
+    auto grow = [](void** p, size_t* have, size_t need) -> cudaError_t {
+        if (*have >= need) return cudaSuccess;
+        if (*p) cudaFree(*p);
+        *p = nullptr;
+        *have = 0;
+        cudaError_t e = cudaMalloc(p, need);
+        if (e == cudaSuccess) *have = need;
+        return e;
+    };
+    cudaError_t e = grow(&st->h_grid, &st->h_grid_bytes, gb);
+    if (e == cudaSuccess) e = grow(&st->h_coef, &st->h_coef_bytes, cb);
+    if (e == cudaSuccess) e = grow(&st->h_ws, &st->h_ws_bytes, gb);
+    if (e != cudaSuccess) return fail(PFSOFT_ENOMEM, std::string("staging allocation: ") + cudaGetErrorString(e));
+    cudaStream_t s = st->h_stream;
+    int rc;
+    if (forward) {
+        PF_CUDA(cudaMemcpyAsync(st->h_grid, in, gb, cudaMemcpyHostToDevice, s));
+        rc = run_dsoft(static_cast<const double*>(st->h_grid), B, static_cast<double*>(st->h_coef), st->h_ws, s);
+        if (rc) return rc;
+        PF_CUDA(cudaMemcpyAsync(out, st->h_coef, cb, cudaMemcpyDeviceToHost, s));
+    } else {
+        PF_CUDA(cudaMemcpyAsync(st->h_coef, in, cb, cudaMemcpyHostToDevice, s));
+        rc = run_idsoft(static_cast<const double*>(st->h_coef), B, static_cast<double*>(st->h_grid), st->h_ws, s);
+        if (rc) return rc;
+        PF_CUDA(cudaMemcpyAsync(out, st->h_grid, gb, cudaMemcpyDeviceToHost, s));
+    }
+    PF_CUDA(cudaStreamSynchronize(s));
+    return PFSOFT_OK;
+}
+
+int pfsoft_dsoft_host(const double* h_grid, int B, double* h_coeffs) { return host_staged(B, true, h_grid, h_coeffs); }
+
+int pfsoft_idsoft_host(const double* h_coeffs, int B, double* h_grid) { return host_staged(B, false, h_coeffs, h_grid); }
+
+static int layer_wise(int cols, int rows, int lays, double* d_arr, double scale, void* stream, int sign)
+{
+    g_last_error.clear();
+    if (cols < 1 || rows < 1 || lays < 1) return fail(PFSOFT_EINVAL, "grid dimensions must be positive");
+    if (cols > 65535 || rows > 65535) return fail(PFSOFT_EINVAL, "layer dimensions above 65535");
+    if (!d_arr) return fail(PFSOFT_EINVAL, "null data pointer");
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    // twiddle tables for both lengths: reuse the bandwidth tables when the length is even
+    // and within range, else build a temporary table
+    double2* G = reinterpret_cast<double2*>(d_arr);
+    const long long r = rows, c = cols, layer = r * c;
+    const int lens[2] = {rows, cols};
+    for (int pass = 0; pass < 2; ++pass) {
+        const int n = lens[pass];
+        const double2* tw = nullptr;
+        void* tmp = nullptr;
+        if (n % 2 == 0 && valid_bandwidth(n / 2)) {
+            BandTables t;
+            int rc = get_tables(n / 2, s, &t);
+            if (rc) return rc;
+            tw = t.twiddle;
+        } else {
+            // odd length: a private table (rare); freed after the stream drains
+            std::vector<double2> h(n);
+            for (int i = 0; i < n; ++i) {
+                const long double a = 6.283185307179586476925286766559005768L * (long double)i / (long double)n;
+                h[i] = make_double2((double)cosl(a), -(double)sinl(a));
+            }
+            PF_CUDA(cudaMalloc(&tmp, n * sizeof(double2)));
+            PF_CUDA(cudaMemcpyAsync(tmp, h.data(), n * sizeof(double2), cudaMemcpyHostToDevice, s));
+            PF_CUDA(cudaStreamSynchronize(s));
+            tw = static_cast<const double2*>(tmp);
+        }
+        FftPassArgs a;
+        memset(&a, 0, sizeof(a));
+        a.n = n;
+        a.kb = kFftKB;
+        a.nstages = fft_plan_radices(n, a.radix, a.ns);
+        a.twiddle = tw;
+        a.scale = pass == 1 ? scale : 1.0;
+        int ntiles;
+        if (pass == 0) {
+            // rows: vectors = layers (stride rows*cols), tile = column index, elements contiguous
+            a.nvec = lays;
+            a.src = a.dst = FftStrides{layer, r, 1};
+            ntiles = cols;
+        } else {
+            // columns: vectors = row index (contiguous), tile = layer, elements stride rows
+            a.nvec = rows;
+            a.src = a.dst = FftStrides{1, layer, r};
+            ntiles = lays;
+        }
+        cudaError_t e = cudaSuccess;
+        if (a.nstages == 0) e = cudaErrorInvalidValue;
+        // grid.y is limited to 65535 tiles: split the launch when needed
+        for (int t0 = 0; e == cudaSuccess && t0 < ntiles; t0 += 65535) {
+            const int nt = ntiles - t0 < 65535 ? ntiles - t0 : 65535;
+            double2* base = G + (long long)t0 * a.src.sb;
+            e = fft_pass_launch(base, base, a, nt, sign, s);
+        }
+        if (tmp) {
+            cudaStreamSynchronize(s);
+            cudaFree(tmp);
+        }
+        if (e != cudaSuccess) return cuda_fail(e, "fft_pass_launch");
+    }
+    return PFSOFT_OK;
+}
+
+int pfsoft_cuda_layer_wise_dft2(int cols, int rows, int lays, double* d_arr, double scale, void* stream)
+{
+    return layer_wise(cols, rows, lays, d_arr, scale, stream, -1);
+}
+
+int pfsoft_cuda_layer_wise_idft2(int cols, int rows, int lays, double* d_arr, double scale, void* stream)
+{
+    return layer_wise(cols, rows, lays, d_arr, scale, stream, +1);
+}
+
+int pfsoft_cuda_quadrature_weights(int B, double* d_w, void* stream)
+{
+    g_last_error.clear();
+    if (!valid_bandwidth(B)) return fail(PFSOFT_EINVAL, "bandwidth must be in [1, 512]");
+    if (!d_w) return fail(PFSOFT_EINVAL, "null output pointer");
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    BandTables t;
+    int rc = get_tables(B, s, &t);
+    if (rc) return rc;
+    copy_weights_kernel<<<(2 * B + 255) / 256, 256, 0, s>>>(t.w, d_w, 2 * B);
+    PF_CUDA(cudaGetLastError());
+    return PFSOFT_OK;
+}
+
+int pfsoft_cuda_wigner_d_matrix(int B, int M, int Mp, int weighted, double* d_out, void* stream)
+{
+    g_last_error.clear();
+    if (!valid_bandwidth(B)) return fail(PFSOFT_EINVAL, "bandwidth must be in [1, 512]");
+    if (!d_out) return fail(PFSOFT_EINVAL, "null output pointer");
+    if (M <= -B || M >= B || Mp <= -B || Mp >= B) return fail(PFSOFT_EINVAL, "orders must satisfy |M|,|M'| < B");
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    BandTables t;
+    int rc = get_tables(B, s, &t);
+    if (rc) return rc;
+    wigner_matrix_kernel<<<(2 * B + 127) / 128, 128, 0, s>>>(B, M, Mp, weighted ? t.w : nullptr, t.cosb, t.sinh,
+                                                              t.cosh, d_out);
+    PF_CUDA(cudaGetLastError());
+    return PFSOFT_OK;
+}
+
+}  // extern "C"

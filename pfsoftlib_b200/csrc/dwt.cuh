@@ -1,0 +1,47 @@
+// Discrete Wigner transform over beta (the DWT stage of DSOFT / iDSOFT), FP64 on CUDA cores.
+#pragma once
+
+#include <cuda_runtime.h>
+
+namespace pfsoft_dev {
+
+// Per-bandwidth constant tables, built once on the device (tables_build) and cached.
+// All doubles; N = 2B, beta_k = pi(2k+1)/(4B) (include/PFSOFTlib_headers/fn_dwt.hpp:155-159).
+struct BandTables {
+    int B = 0, N = 0;
+    double* cosb = nullptr;     // cos(beta_k)                    [N]
+    double* sinh = nullptr;     // sin(beta_k / 2)                [N]
+    double* cosh = nullptr;     // cos(beta_k / 2)                [N]
+    double* w = nullptr;        // quadrature weights w_B(k)      [N]   (fn_dwt.hpp:62-83)
+    double* normf = nullptr;    // seed norm per order class      [B(B+1)/2] (fn_dwt.hpp:117-121)
+    double2* twiddle = nullptr; // exp(-2 pi i t / N)             [N]
+    void* block = nullptr;      // single allocation holding all of the above
+};
+
+size_t tables_bytes(int B);
+// Carve the tables out of `mem` (tables_bytes(B) bytes, 256-byte aligned) and fill them.
+cudaError_t tables_build(int B, void* mem, BandTables* t, cudaStream_t stream);
+
+struct DwtArgs {
+    int B, N;
+    const double* cosb;
+    const double* sinh;
+    const double* cosh;
+    const double* w;
+    const double* normf;
+    int team_warps;   // warps cooperating on one order class (1..4)
+};
+
+// Forward: X (beta-innermost spectrum, N^3) -> packed coefficients, scale pi/(2B^2).
+cudaError_t dwt_forward_launch(const double2* X, double2* coeffs, const DwtArgs& a, int nblocks,
+                               cudaStream_t stream);
+// Inverse: packed coefficients -> X (all non-Nyquist beta columns), scale 2B^2/pi.
+cudaError_t dwt_inverse_launch(const double2* coeffs, double2* X, const DwtArgs& a, int nblocks,
+                               cudaStream_t stream);
+// Zero the beta columns of the Nyquist bins (row == B or col == B) of X.
+cudaError_t zero_nyquist_launch(double2* X, int B, cudaStream_t stream);
+
+// Team shape for a bandwidth: warps per class so that each lane owns at most 4 beta columns.
+int dwt_team_warps(int N);
+
+}  // namespace pfsoft_dev

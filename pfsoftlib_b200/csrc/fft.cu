@@ -1,0 +1,339 @@
+// Batched 1D DFT passes over the (alpha, gamma) plane of every beta layer (sm_100a).
+//
+// Algorithm: mixed-radix Stockham autosort (Govindaraju et al., SC'08 formulation). A stage of
+// radix R over n points with Ns = product of the earlier radices maps butterfly j to
+//   inputs  x[j + r*n/R] * w_n^(r * (j mod Ns) * n/(Ns R)),   r < R
+//   outputs y[(j/Ns)*Ns*R + (j mod Ns) + q*Ns],              q < R
+// and the last stage leaves the result in natural order. The first stage reads HBM directly
+// into registers and the last stage writes HBM directly from registers; the stages between
+// exchange through shared memory (ping-pong buffers). Radices 2, 4, 8, 16, 3, 5 have
+// register butterflies; any other prime uses a direct O(R^2) butterfly.
+//
+// Coalescing: each stage picks its butterfly -> thread map from the stride of the HBM side
+// it touches. If consecutive elements of a vector are contiguous in HBM (se == 1) threads run
+// along the vector; otherwise threads run across the KB vectors of the tile, whose values are
+// contiguous (sv == 1), so KB*16 bytes move per group of KB lanes. That is how the beta <->
+// (alpha, gamma) transpose rides inside the first and last stage at no extra HBM traffic.
+
+#include "common.cuh"
+#include "fft.cuh"
+
+namespace pfsoft_dev {
+
+namespace {
+
+constexpr double kSqrtHalf = 0.70710678118654752440084436210485;
+constexpr double kCosPi8 = 0.92387953251128675612818318939679;   // cos(pi/8)
+constexpr double kSinPi8 = 0.38268343236508977172845998403040;   // sin(pi/8)
+constexpr double kSin60 = 0.86602540378443864676372317075294;    // sin(pi/3)
+constexpr double kC5_1 = 0.30901699437494742410229341718282;     // cos(2pi/5)
+constexpr double kC5_2 = -0.80901699437494742410229341718282;    // cos(4pi/5)
+constexpr double kS5_1 = 0.95105651629515357211643933337938;     // sin(2pi/5)
+constexpr double kS5_2 = 0.58778525229247312916870595463907;     // sin(4pi/5)
+
+template <int SIGN>
+__device__ __forceinline__ void dft2(double2* v)
+{
+    double2 a = v[0], b = v[1];
+    v[0] = cadd(a, b);
+    v[1] = csub(a, b);
+}
+
+template <int SIGN>
+__device__ __forceinline__ void dft4(double2& v0, double2& v1, double2& v2, double2& v3)
+{
+    double2 a0 = cadd(v0, v2), a1 = csub(v0, v2);
+    double2 b0 = cadd(v1, v3), b1 = cmul_i<SIGN>(csub(v1, v3));
+    v0 = cadd(a0, b0);
+    v2 = csub(a0, b0);
+    v1 = cadd(a1, b1);
+    v3 = csub(a1, b1);
+}
+
+// w8^q = exp(SIGN*2*pi*i*q/8)
+template <int SIGN, int Q>
+__device__ __forceinline__ double2 rot8(double2 a)
+{
+    if (Q == 0) return a;
+    if (Q == 2) return cmul_i<SIGN>(a);
+    if (Q == 1) return make_double2(kSqrtHalf * (a.x - SIGN * a.y), kSqrtHalf * (a.y + SIGN * a.x));
+    // Q == 3: (-1 + SIGN i)/sqrt2
+    return make_double2(kSqrtHalf * (-a.x - SIGN * a.y), kSqrtHalf * (-a.y + SIGN * a.x));
+}
+
+template <int SIGN>
+__device__ __forceinline__ void dft8(double2* v)
+{
+    // even/odd split: E = DFT4(v0 v2 v4 v6), O = DFT4(v1 v3 v5 v7)
+    dft4<SIGN>(v[0], v[2], v[4], v[6]);
+    dft4<SIGN>(v[1], v[3], v[5], v[7]);
+    double2 o1 = rot8<SIGN, 1>(v[3]), o2 = rot8<SIGN, 2>(v[5]), o3 = rot8<SIGN, 3>(v[7]);
+    double2 e0 = v[0], e1 = v[2], e2 = v[4], e3 = v[6], o0 = v[1];
+    v[0] = cadd(e0, o0);
+    v[4] = csub(e0, o0);
+    v[1] = cadd(e1, o1);
+    v[5] = csub(e1, o1);
+    v[2] = cadd(e2, o2);
+    v[6] = csub(e2, o2);
+    v[3] = cadd(e3, o3);
+    v[7] = csub(e3, o3);
+}
+
+template <int SIGN>
+__device__ __forceinline__ void dft16(double2* v)
+{
+    double2 e[8], o[8];
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+        e[i] = v[2 * i];
+        o[i] = v[2 * i + 1];
+    }
+    dft8<SIGN>(e);
+    dft8<SIGN>(o);
+    // w16^q = (cos(pi q/8), SIGN sin(pi q/8))
+    const double cq[8] = {1.0, kCosPi8, kSqrtHalf, kSinPi8, 0.0, -kSinPi8, -kSqrtHalf, -kCosPi8};
+    const double sq[8] = {0.0, kSinPi8, kSqrtHalf, kCosPi8, 1.0, kCosPi8, kSqrtHalf, kSinPi8};
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+        double2 t = (q == 0) ? o[0] : make_double2(cq[q] * o[q].x - SIGN * sq[q] * o[q].y,
+                                                    cq[q] * o[q].y + SIGN * sq[q] * o[q].x);
+        v[q] = cadd(e[q], t);
+        v[q + 8] = csub(e[q], t);
+    }
+}
+
+template <int SIGN>
+__device__ __forceinline__ void dft3(double2* v)
+{
+    double2 t1 = cadd(v[1], v[2]);
+    double2 t2 = csub(v[1], v[2]);
+    double2 a = make_double2(v[0].x - 0.5 * t1.x, v[0].y - 0.5 * t1.y);
+    double2 b = cmul_i<SIGN>(cscale(t2, kSin60));
+    v[0] = cadd(v[0], t1);
+    v[1] = cadd(a, b);
+    v[2] = csub(a, b);
+}
+
+template <int SIGN>
+__device__ __forceinline__ void dft5(double2* v)
+{
+    double2 t1 = cadd(v[1], v[4]), t2 = cadd(v[2], v[3]);
+    double2 t3 = csub(v[1], v[4]), t4 = csub(v[2], v[3]);
+    double2 a1 = make_double2(v[0].x + kC5_1 * t1.x + kC5_2 * t2.x, v[0].y + kC5_1 * t1.y + kC5_2 * t2.y);
+    double2 a2 = make_double2(v[0].x + kC5_2 * t1.x + kC5_1 * t2.x, v[0].y + kC5_2 * t1.y + kC5_1 * t2.y);
+    double2 b1 = cmul_i<SIGN>(make_double2(kS5_1 * t3.x + kS5_2 * t4.x, kS5_1 * t3.y + kS5_2 * t4.y));
+    double2 b2 = cmul_i<SIGN>(make_double2(kS5_2 * t3.x - kS5_1 * t4.x, kS5_2 * t3.y - kS5_1 * t4.y));
+    v[0] = cadd(v[0], cadd(t1, t2));
+    v[1] = cadd(a1, b1);
+    v[4] = csub(a1, b1);
+    v[2] = cadd(a2, b2);
+    v[3] = csub(a2, b2);
+}
+
+__device__ __forceinline__ double2 twiddle(const double2* __restrict__ tw, int t, int sign)
+{
+    double2 w = __ldg(tw + t);
+    return sign < 0 ? w : make_double2(w.x, -w.y);
+}
+
+// smem position of element i of a vector (one pad slot every 16 elements)
+__device__ __forceinline__ int spos(int i) { return i + (i >> 4); }
+
+__host__ __device__ __forceinline__ int padded_len(int n) { return n + (n >> 4) + 1; }
+
+template <int SIGN, int R>
+__device__ __forceinline__ void run_stage_fixed(const FftPassArgs& a, int s, const double2* gsrc,
+                                                double2* gdst, const double2* sin_, double2* sout,
+                                                int nv, long long src_base, long long dst_base)
+{
+    const int n = a.n;
+    const int m = n / R;
+    const int Ns = a.ns[s];
+    const int step = n / (Ns * R);
+    const bool first = (s == 0), last = (s == a.nstages - 1);
+    const int pl = padded_len(n);
+    // thread map: along the vector (j fastest) unless this stage touches HBM with a non-unit
+    // element stride, in which case across vectors (kk fastest)
+    const bool kk_fast = (first && a.src.se != 1) || (last && a.dst.se != 1);
+    const int total = nv * m;
+    for (int t = threadIdx.x; t < total; t += blockDim.x) {
+        int j, kk;
+        if (kk_fast) {
+            kk = t % nv;
+            j = t / nv;
+        } else {
+            j = t % m;
+            kk = t / m;
+        }
+        double2 v[R];
+        if (first) {
+            const double2* p = gsrc + src_base + (long long)kk * a.src.sv;
+#pragma unroll
+            for (int r = 0; r < R; ++r) v[r] = __ldg(p + (long long)(j + r * m) * a.src.se);
+        } else {
+            const double2* p = sin_ + kk * pl;
+#pragma unroll
+            for (int r = 0; r < R; ++r) v[r] = p[spos(j + r * m)];
+        }
+        const int k = j % Ns;
+        if (Ns > 1) {
+#pragma unroll
+            for (int r = 1; r < R; ++r) v[r] = cmul(v[r], twiddle(a.twiddle, r * k * step, SIGN));
+        }
+        if (R == 2) dft2<SIGN>(v);
+        else if (R == 4) dft4<SIGN>(v[0], v[1], v[2], v[3]);
+        else if (R == 8) dft8<SIGN>(v);
+        else if (R == 16) dft16<SIGN>(v);
+        else if (R == 3) dft3<SIGN>(v);
+        else if (R == 5) dft5<SIGN>(v);
+        const int ob = (j / Ns) * Ns * R + k;
+        if (last) {
+            double2* p = gdst + dst_base + (long long)kk * a.dst.sv;
+#pragma unroll
+            for (int q = 0; q < R; ++q) p[(long long)(ob + q * Ns) * a.dst.se] = cscale(v[q], a.scale);
+        } else {
+            double2* p = sout + kk * pl;
+#pragma unroll
+            for (int q = 0; q < R; ++q) p[spos(ob + q * Ns)] = v[q];
+        }
+    }
+}
+
+// Direct O(R^2) butterfly for any other radix (rare lengths with a large prime factor).
+template <int SIGN>
+__device__ void run_stage_generic(const FftPassArgs& a, int s, const double2* gsrc,
+                                  double2* gdst, const double2* sin_, double2* sout, int nv,
+                                  long long src_base, long long dst_base)
+{
+    const int n = a.n, R = a.radix[s];
+    const int m = n / R;
+    const int Ns = a.ns[s];
+    const int step = n / (Ns * R);
+    const int rstep = n / R;   // exp(SIGN 2 pi i rq/R) = twiddle[(rq mod R) * n/R]
+    const bool first = (s == 0), last = (s == a.nstages - 1);
+    const int pl = padded_len(n);
+    const bool kk_fast = (first && a.src.se != 1) || (last && a.dst.se != 1);
+    const int total = nv * m;
+    for (int t = threadIdx.x; t < total; t += blockDim.x) {
+        int j, kk;
+        if (kk_fast) {
+            kk = t % nv;
+            j = t / nv;
+        } else {
+            j = t % m;
+            kk = t / m;
+        }
+        const int k = j % Ns;
+        const int ob = (j / Ns) * Ns * R + k;
+        for (int q = 0; q < R; ++q) {
+            double2 acc = make_double2(0.0, 0.0);
+            for (int r = 0; r < R; ++r) {
+                double2 x = first ? __ldg(gsrc + src_base + (long long)kk * a.src.sv + (long long)(j + r * m) * a.src.se)
+                                  : sin_[kk * pl + spos(j + r * m)];
+                if (Ns > 1 && r > 0) x = cmul(x, twiddle(a.twiddle, r * k * step, SIGN));
+                const int e = (r * q) % R;
+                if (e) x = cmul(x, twiddle(a.twiddle, e * rstep, SIGN));
+                acc = cadd(acc, x);
+            }
+            if (last) gdst[dst_base + (long long)kk * a.dst.sv + (long long)(ob + q * Ns) * a.dst.se] = cscale(acc, a.scale);
+            else sout[kk * pl + spos(ob + q * Ns)] = acc;
+        }
+    }
+}
+
+template <int SIGN>
+__global__ void __launch_bounds__(256) fft_pass_kernel(const double2* src, double2* dst,
+                                                       const FftPassArgs a)
+{
+    extern __shared__ double2 smem[];
+    const int v0 = blockIdx.x * a.kb;
+    const int nv = min(a.kb, a.nvec - v0);
+    const long long src_base = (long long)v0 * a.src.sv + (long long)blockIdx.y * a.src.sb;
+    const long long dst_base = (long long)v0 * a.dst.sv + (long long)blockIdx.y * a.dst.sb;
+    const int pl = padded_len(a.n);
+    double2* buf[2] = {smem, smem + a.kb * pl};
+    // In-place passes (src == dst) are safe: every CTA reads its whole tile in stage 0 and
+    // writes it only in the last stage, after at least one __syncthreads (nstages >= 2), or in
+    // the same thread's registers when there is a single stage.
+    for (int s = 0; s < a.nstages; ++s) {
+        const double2* sin_ = buf[(s + 1) & 1];
+        double2* sout = buf[s & 1];
+        switch (a.radix[s]) {
+            case 16: run_stage_fixed<SIGN, 16>(a, s, src, dst, sin_, sout, nv, src_base, dst_base); break;
+            case 8: run_stage_fixed<SIGN, 8>(a, s, src, dst, sin_, sout, nv, src_base, dst_base); break;
+            case 4: run_stage_fixed<SIGN, 4>(a, s, src, dst, sin_, sout, nv, src_base, dst_base); break;
+            case 2: run_stage_fixed<SIGN, 2>(a, s, src, dst, sin_, sout, nv, src_base, dst_base); break;
+            case 3: run_stage_fixed<SIGN, 3>(a, s, src, dst, sin_, sout, nv, src_base, dst_base); break;
+            case 5: run_stage_fixed<SIGN, 5>(a, s, src, dst, sin_, sout, nv, src_base, dst_base); break;
+            default: run_stage_generic<SIGN>(a, s, src, dst, sin_, sout, nv, src_base, dst_base); break;
+        }
+        if (s + 1 < a.nstages) __syncthreads();
+    }
+}
+
+}  // namespace
+
+int fft_plan_radices(int n, int* radix, int* ns)
+{
+    if (n < 1) return 0;
+    int r[64];
+    int cnt = 0, rem = n;
+    int p2 = 0;
+    while (rem % 2 == 0) {
+        rem /= 2;
+        ++p2;
+    }
+    // power-of-two part in radix-16 stages, remainder folded into one or two smaller stages
+    int q = p2 / 4, rr = p2 % 4;
+    if (rr == 1 && q > 0) {
+        --q;
+        r[cnt++] = 8;
+        r[cnt++] = 4;
+    } else if (rr == 1) {
+        r[cnt++] = 2;
+    } else if (rr == 2) {
+        r[cnt++] = 4;
+    } else if (rr == 3) {
+        r[cnt++] = 8;
+    }
+    for (int i = 0; i < q; ++i) r[cnt++] = 16;
+    while (rem % 3 == 0) { r[cnt++] = 3; rem /= 3; }
+    while (rem % 5 == 0) { r[cnt++] = 5; rem /= 5; }
+    for (int p = 7; rem > 1; p += 2) {
+        while (rem % p == 0) { r[cnt++] = p; rem /= p; }
+    }
+    if (cnt == 0) r[cnt++] = 1;
+    if (cnt > kFftMaxStages) return 0;
+    int nsv = 1;
+    for (int i = 0; i < cnt; ++i) {
+        radix[i] = r[i];
+        ns[i] = nsv;
+        nsv *= r[i];
+    }
+    return cnt;
+}
+
+size_t fft_pass_smem_bytes(const FftPassArgs& a)
+{
+    const int buffers = a.nstages >= 3 ? 2 : (a.nstages == 2 ? 1 : 0);
+    return (size_t)buffers * a.kb * padded_len(a.n) * sizeof(double2);
+}
+
+cudaError_t fft_pass_launch(const double2* src, double2* dst, const FftPassArgs& a, int ntiles, int sign,
+                            cudaStream_t stream)
+{
+    const int nthreads = 256;
+    dim3 grid((a.nvec + a.kb - 1) / a.kb, ntiles);
+    size_t smem = fft_pass_smem_bytes(a);
+    // the kernel indexes two buffers; with a single buffer the second pointer is never used
+    if (sign < 0) {
+        if (smem > 48 * 1024) cudaFuncSetAttribute(fft_pass_kernel<-1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        fft_pass_kernel<-1><<<grid, nthreads, smem, stream>>>(src, dst, a);
+    } else {
+        if (smem > 48 * 1024) cudaFuncSetAttribute(fft_pass_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        fft_pass_kernel<1><<<grid, nthreads, smem, stream>>>(src, dst, a);
+    }
+    return cudaGetLastError();
+}
+
+}  // namespace pfsoft_dev

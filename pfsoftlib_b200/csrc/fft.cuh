@@ -1,0 +1,39 @@
+// Batched layer-wise 2D DFT passes (the reference's uzl_fftw_layer_wise_{DFT2,IDFT2}_grid3D,
+// src/fftw_wrapper.cpp:47-173, re-designed for HBM): each pass is one 1D DFT direction over
+// every beta layer, tiled so that one CTA transforms KB vectors, with the transpose to or from
+// the beta-innermost spectrum layout fused into the load or store.
+#pragma once
+
+#include <cuda_runtime.h>
+
+namespace pfsoft_dev {
+
+constexpr int kFftMaxStages = 12;
+
+// Element e of vector v in tile b lives at  base + v*sv + b*sb + e*se  (units of double2).
+struct FftStrides {
+    long long sv, sb, se;
+};
+
+struct FftPassArgs {
+    int n;                       // transform length
+    int nvec;                    // total vectors along the tiled index (k)
+    int kb;                      // vectors per CTA
+    int nstages;
+    int radix[kFftMaxStages];
+    int ns[kFftMaxStages];       // product of the radices of the earlier stages
+    FftStrides src, dst;
+    double scale;                // applied to the stored values (1 = none)
+    const double2* twiddle;      // twiddle[t] = exp(-2*pi*i*t/n), t < n
+};
+
+// Radix plan for length n; returns the number of stages (0 if n cannot be planned).
+int fft_plan_radices(int n, int* radix, int* ns);
+
+// Launch one pass over a grid of (ceil(nvec/kb), ntiles) CTAs. sign = -1 forward, +1 inverse.
+cudaError_t fft_pass_launch(const double2* src, double2* dst, const FftPassArgs& a, int ntiles, int sign,
+                            cudaStream_t stream);
+
+size_t fft_pass_smem_bytes(const FftPassArgs& a);
+
+}  // namespace pfsoft_dev
