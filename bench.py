@@ -1,0 +1,361 @@
+"""Benchmark: DSOFT + iDSOFT transforms/s at bandwidth B = 128 (one B200 per rank).
+
+One step = one iDSOFT (2,796,160 coefficients -> 256^3 complex128 grid) followed by one DSOFT
+of that grid (the single-transform workload at B = 128), i.e. 2 transforms per step. Inputs are
+seeded synthetic coefficients: uniform phase, magnitude (1+l)^-1 |N(0,1)|, PCG64 seed 1.
+
+  value     transforms/s with everything resident in HBM, device time (CUDA events) over the
+            K timed steps, max over ranks; every buffer (268 MB grid) exceeds the 126 MB L2.
+  e2e       the same metric through the host-facing C ABI (pfsoft_idsoft_host /
+            pfsoft_dsoft_host) from pinned host memory, copies inside the timed region.
+  roofline  the dominant stage, timed with CUDA events per stage inside the timed region.
+  cpu_baseline  the reference's own CPU DSOFT/IDSOFT (compiled from its sources with a project
+            FFT in FFTW's place) on a bounded sample, rank 0 at N = 1 only.
+
+--impl reference times the reference CPU implementation alone on the host cores.
+Multi-GPU (torchrun): every rank runs its own transforms (independent replicas, weak scaling);
+no collective touches the data path.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+B = 128
+N = 2 * B
+METRIC = "DSOFT+iDSOFT transforms/s at B=128"
+UNIT = "transforms/s"
+TRANSFORMS_PER_STEP = 2
+GRID_BYTES = N ** 3 * 16
+COEF_COUNT = B * (4 * B * B - 1) // 3
+COEF_BYTES = COEF_COUNT * 16
+FP64_PEAK_TFLOPS = 37.0   # mma.sync m8n8k4 f64 on this pool's B200 (DFMA measured 33.5)
+
+# algorithmic work per transform (see DESIGN.md "Roofline"):
+#   each FFT pass reads and writes the grid once: 32 N^3 bytes
+#   each DWT does 8 B^2 (4B^2-1)/3 useful FP64 flops
+FFT_PASS_BYTES = 2 * GRID_BYTES
+DWT_FLOPS = 8 * B * B * (4 * B * B - 1) / 3
+
+
+def workload_config(l2_note: str) -> dict:
+    return {
+        "workload": "single transform at B=128: iDSOFT of 2,796,160 complex128 coefficients to a "
+                    "256^3 complex128 grid, then DSOFT of that grid",
+        "B": B,
+        "grid": "256x256x256 complex128 (268 MB)",
+        "coefficients": COEF_COUNT,
+        "transforms_per_step": TRANSFORMS_PER_STEP,
+        "inputs": "seeded synthetic (PCG64 seed 1): uniform phase, |f| = (1+l)^-1 |N(0,1)|",
+        "l2": l2_note,
+    }
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="pfsoft", choices=["pfsoft", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def dist_env():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+# ----------------------------------------------------------------------------- clocks
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms during the timed region."""
+
+    FIELDS = "index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active," \
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown," \
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap"
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.f = None
+
+    def start(self):
+        try:
+            self.f = tempfile.NamedTemporaryFile(mode="w+", suffix=".csv", delete=False)
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=self.f, stderr=subprocess.DEVNULL)
+        except (OSError, FileNotFoundError):
+            self.proc = None
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.f.flush()
+        self.f.seek(0)
+        rows = [r.split(",") for r in self.f.read().strip().splitlines() if r.strip()]
+        self.f.close()
+        os.unlink(self.f.name)
+        sm, smax, reasons, power = [], [], set(), []
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            try:
+                sm.append(float(r[1]))
+                smax.append(float(r[2]))
+                power.append(float(r[3]))
+                for i, nm in enumerate(names):
+                    if r[5 + i].strip().lower() == "active":
+                        reasons.add(nm)
+            except (ValueError, IndexError):
+                continue
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "power_w_max": max(power) if power else None, "samples": len(sm), "reasons": sorted(reasons)}
+
+
+# ----------------------------------------------------------------------------- reference arm
+
+def cpu_reference_sample(steps: int, warmup: int, coeffs) -> dict:
+    """Times the reference CPU DSOFT/IDSOFT (all host threads) at B = 128."""
+    from oracle import oracle as orc
+
+    if orc.Reference.available():
+        ref = orc.Reference()
+        kind = "reference"
+        threads = ref.max_threads()
+        timer = orc.ReferenceTimer(ref, B, coeffs)
+        for _ in range(warmup):
+            timer.idsoft(threads)
+            timer.dsoft(threads)
+        t = 0.0
+        for _ in range(steps):
+            t += timer.idsoft(threads)
+            t += timer.dsoft(threads)
+        timer.close()
+        sample = (f"{steps} x (IDSOFT + DSOFT) at B=128 after {warmup} warm-up, reference sources "
+                  f"compiled -O3 -fopenmp with the project FFT in FFTW's slot; timing as "
+                  f"benchmark/benchmark_dsoft_for.cpp (by-value grid copy included)")
+    else:
+        ora = orc.Oracle()
+        kind = "port"
+        threads = os.cpu_count() or 1
+        t0 = time.perf_counter()
+        g = ora.idsoft(coeffs, B)
+        ora.dsoft(g)
+        t = time.perf_counter() - t0
+        steps = 1
+        sample = "1 x (IDSOFT + DSOFT) at B=128 through the long-double C restatement (oracle/)"
+    return {"value": TRANSFORMS_PER_STEP * steps / t, "unit": UNIT, "cores": threads, "kind": kind,
+            "sample": sample, "seconds": t}
+
+
+def run_reference_arm(args):
+    rank, world, _ = dist_env()
+    if rank != 0:
+        return
+    from oracle import oracle as orc
+
+    coeffs = orc.coeffs_decaying(B, seed=1, power=1.0, normal_mag=True)
+    steps = max(1, min(args.steps, 20))
+    warm = 1 if args.warmup > 0 else 0
+    cb = cpu_reference_sample(steps, warm, coeffs)
+    line = {
+        "impl": "reference", "metric": METRIC, "value": cb["value"], "unit": UNIT, "n_gpus": args.gpus,
+        "steps": steps, "warmup": warm, "ms_per_step": 1e3 * cb["seconds"] / steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64 (long double DWT accumulation)", "data": "synthetic",
+        "config": workload_config("host memory"),
+        "cpu_baseline": {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")},
+        "e2e": {"value": cb["value"], "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+# ----------------------------------------------------------------------------- GPU arm
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference_arm(args)
+        return
+
+    import numpy as np
+    import torch
+
+    import pfsoftlib_b200
+    from oracle import oracle as orc
+
+    rank, world, local = dist_env()
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+
+    lib = pfsoftlib_b200.load()
+    stream = torch.cuda.current_stream()
+    sp = stream.cuda_stream
+
+    coeffs_h = orc.coeffs_decaying(B, seed=1, power=1.0, normal_mag=True)
+    c = torch.from_numpy(coeffs_h).cuda()
+    f = torch.empty_like(c)
+    g = torch.empty((N, N, N), dtype=torch.complex128, device="cuda")
+    ws = torch.empty(lib.pfsoft_workspace_bytes(B) // 8, dtype=torch.float64, device="cuda")
+    wp, wb = ws.data_ptr(), ws.numel() * 8
+
+    def step():
+        rc = lib.pfsoft_cuda_idsoft(c.data_ptr(), B, g.data_ptr(), wp, wb, sp)
+        rc |= lib.pfsoft_cuda_dsoft(g.data_ptr(), B, f.data_ptr(), wp, wb, sp)
+        if rc:
+            raise RuntimeError(lib.pfsoft_last_error().decode())
+
+    def barrier():
+        torch.cuda.synchronize()
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    for _ in range(max(3, args.warmup)):
+        step()
+    barrier()
+
+    # ---- timed region (device time) with per-stage events. The clock sampler runs from
+    # here; extra untimed steps keep the GPU loaded for >= 0.6 s before the timed region so
+    # that the 200 ms sampler sees the load even when the timed region itself is short.
+    clocks = ClockSampler(local)
+    clocks.start()
+    t_load = time.perf_counter()
+    while time.perf_counter() - t_load < 0.6:
+        step()
+        torch.cuda.synchronize()
+    lib.pfsoft_profile_read(None, None, 0)
+    lib.pfsoft_profile_enable(1)
+    launches0 = lib.pfsoft_launch_count()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    barrier()
+    e0.record(stream)
+    for _ in range(args.steps):
+        step()
+    e1.record(stream)
+    barrier()
+    launches = lib.pfsoft_launch_count() - launches0
+    lib.pfsoft_profile_enable(0)
+    nst = 16
+    st_ms = np.zeros(nst)
+    st_cnt = np.zeros(nst, dtype=np.int64)
+    nstages = lib.pfsoft_profile_read(st_ms.ctypes.data, st_cnt.ctypes.data, nst)
+    clk = clocks.stop()
+    ms = e0.elapsed_time(e1)
+    if dist is not None:
+        t = torch.tensor([ms], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    value = TRANSFORMS_PER_STEP * args.steps * world / (ms / 1e3)
+
+    # ---- accuracy of the timed results (round trip at B = 128)
+    f_h = f.cpu().numpy()
+    acc = {"round_trip_rel_l2": orc.rel_l2(f_h, coeffs_h), "round_trip_max_abs": orc.max_abs(f_h, coeffs_h)}
+
+    # ---- per-stage roofline
+    stages = {}
+    for i in range(nstages):
+        name = lib.pfsoft_profile_stage_name(i).decode()
+        if st_cnt[i] == 0:
+            continue
+        per = st_ms[i] / st_cnt[i]
+        if name.startswith("fft"):
+            achieved = FFT_PASS_BYTES / (per / 1e3) / 1e9
+            stages[name] = {"bound": "hbm", "ms_per_launch": per, "launches": int(st_cnt[i]),
+                            "achieved": achieved, "peak": 6551.7, "unit": "GB/s", "frac": achieved / 6551.7}
+        elif name.startswith("dwt"):
+            achieved = DWT_FLOPS / (per / 1e3) / 1e12
+            stages[name] = {"bound": "tensor", "ms_per_launch": per, "launches": int(st_cnt[i]),
+                            "achieved": achieved, "peak": FP64_PEAK_TFLOPS, "unit": "TFLOP/s",
+                            "frac": achieved / FP64_PEAK_TFLOPS}
+        else:
+            stages[name] = {"ms_per_launch": per, "launches": int(st_cnt[i])}
+    dominant = max((k for k in stages if "frac" in stages[k]), key=lambda k: stages[k]["ms_per_launch"] * stages[k]["launches"])
+    d = stages[dominant]
+    traffic = {"dwt_forward": None, "dwt_inverse": None}
+    roofline = {"kernel": dominant, "bound": d["bound"], "achieved": d["achieved"], "peak": d["peak"],
+                "unit": d["unit"], "frac": d["frac"], "traffic": traffic.get(dominant),
+                "peak_source": ("measured FP64 MMA peak (own micro-benchmark; MEASURED_PEAKS.json has no FP64 entry)"
+                                if d["bound"] == "tensor" else "measured copy bandwidth, MEASURED_PEAKS.json hbm_gbs")}
+
+    # ---- end to end through the host-facing C ABI (pinned host buffers)
+    ch = torch.from_numpy(coeffs_h).pin_memory()
+    gh = torch.empty((N, N, N), dtype=torch.complex128).pin_memory()
+    fh = torch.empty_like(ch).pin_memory()
+    e2e_steps = max(2, min(args.steps, 10))
+
+    def host_step():
+        rc = lib.pfsoft_idsoft_host(ch.data_ptr(), B, gh.data_ptr())
+        rc |= lib.pfsoft_dsoft_host(gh.data_ptr(), B, fh.data_ptr())
+        if rc:
+            raise RuntimeError(lib.pfsoft_last_error().decode())
+
+    host_step()
+    barrier()
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        host_step()
+    t_e2e = time.perf_counter() - t0
+    if dist is not None:
+        t = torch.tensor([t_e2e], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        t_e2e = float(t.item())
+    e2e = {"value": TRANSFORMS_PER_STEP * e2e_steps * world / t_e2e, "unit": UNIT,
+           "h2d_bytes_per_step": COEF_BYTES + GRID_BYTES, "d2h_bytes_per_step": GRID_BYTES + COEF_BYTES,
+           "api": "pfsoft_idsoft_host + pfsoft_dsoft_host (include/pfsoft_b200.h), pinned host buffers", "steps": e2e_steps}
+
+    # ---- CPU baseline (rank 0, N = 1 only)
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cb = cpu_reference_sample(1, 0, coeffs_h)
+        cpu = {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")}
+        # parity of the GPU DSOFT against the reference DSOFT of the same grid
+        if cb["kind"] == "reference":
+            ref = orc.Reference()
+            g_h = g.cpu().numpy()
+            f_ref = ref.dsoft(g_h, ref.max_threads())
+            acc["vs_reference_dsoft_rel_l2"] = orc.rel_l2(f_h, f_ref)
+            acc["vs_reference_dsoft_max_abs"] = orc.max_abs(f_h, f_ref)
+
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank != 0:
+        return
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": max(3, args.warmup), "ms_per_step": ms / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": workload_config("inputs larger than L2: 268 MB grid and workspace, 45 MB coefficients"),
+        "e2e": e2e, "gpu_launches": int(launches), "roofline": roofline, "stages": stages,
+        "cpu_baseline": cpu, "accuracy": acc, "clocks": clk,
+        "parallelism": f"replicas x{world} (independent transforms per GPU, no collective)",
+    }
+    print(json.dumps(line), flush=True)
+
+
+if __name__ == "__main__":
+    main()

@@ -93,6 +93,20 @@ int pfsoft_cuda_layer_wise_idft2(int cols, int rows, int lays, double* d_arr, do
 int pfsoft_cuda_quadrature_weights(int B, double* d_w, void* stream);
 int pfsoft_cuda_wigner_d_matrix(int B, int M, int Mp, int weighted, double* d_out, void* stream);
 
+/* ---- Diagnostics (no counterpart in the reference) -----------------------------------------
+ * pfsoft_launch_count: number of CUDA kernels this library has launched in the process.
+ * pfsoft_profile_enable(1) brackets every stage the library launches with CUDA events on the
+ * stage's stream; pfsoft_profile_read() waits for them and returns, per stage, the summed
+ * device milliseconds and launch count (and resets them). Returns the number of stages;
+ * pfsoft_profile_stage_name(i) names stage i. */
+long long pfsoft_launch_count(void);
+/* Tuning knob used by the autotuner: direction 0 = DSOFT, 1 = IDSOFT; case_split 1 = each warp
+ * applies all eight symmetry cases, 2 = warp pairs split them, 0 = library default. */
+int pfsoft_tune_dwt_case_split(int direction, int case_split);
+int pfsoft_profile_enable(int on);
+int pfsoft_profile_read(double* ms, long long* launches, int max_stages);
+const char* pfsoft_profile_stage_name(int stage);
+
 #ifdef __cplusplus
 }
 #endif

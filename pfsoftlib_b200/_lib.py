@@ -32,6 +32,11 @@ SIGNATURES = {
     "pfsoft_cuda_layer_wise_idft2": (_c_int, [_c_int, _c_int, _c_int, _vp, _c_double, _vp]),
     "pfsoft_cuda_quadrature_weights": (_c_int, [_c_int, _vp, _vp]),
     "pfsoft_cuda_wigner_d_matrix": (_c_int, [_c_int, _c_int, _c_int, _c_int, _vp, _vp]),
+    "pfsoft_launch_count": (ctypes.c_longlong, []),
+    "pfsoft_tune_dwt_case_split": (_c_int, [_c_int, _c_int]),
+    "pfsoft_profile_enable": (_c_int, [_c_int]),
+    "pfsoft_profile_read": (_c_int, [_vp, _vp, _c_int]),
+    "pfsoft_profile_stage_name": (ctypes.c_char_p, [_c_int]),
 }
 
 

@@ -11,6 +11,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <atomic>
 #include <map>
 #include <mutex>
 #include <string>
@@ -74,6 +75,60 @@ DeviceState* device_state(int dev)
     return s;
 }
 
+// ---- launch accounting and optional per-stage timing ------------------------------------
+enum Stage { ST_FFT_FWD_ROWS, ST_FFT_FWD_COLS, ST_DWT_FWD, ST_NYQUIST, ST_DWT_INV, ST_FFT_INV_COLS, ST_FFT_INV_ROWS,
+             ST_TABLES, ST_COUNT };
+const char* kStageNames[ST_COUNT] = {"fft_forward_gamma", "fft_forward_alpha", "dwt_forward", "zero_nyquist",
+                                     "dwt_inverse", "fft_inverse_alpha", "fft_inverse_gamma", "tables"};
+
+std::atomic<long long> g_launches{0};
+
+struct Profiler {
+    std::mutex mu;
+    bool on = false;
+    struct Rec { int stage; cudaEvent_t a, b; };
+    std::vector<Rec> recs;
+    std::vector<cudaEvent_t> pool;
+    double ms[ST_COUNT] = {0};
+    long long count[ST_COUNT] = {0};
+
+    cudaEvent_t ev()
+    {
+        if (!pool.empty()) {
+            cudaEvent_t e = pool.back();
+            pool.pop_back();
+            return e;
+        }
+        cudaEvent_t e = nullptr;
+        cudaEventCreate(&e);
+        return e;
+    }
+} g_prof;
+
+// Brackets one stage launch: counts it, and times it when profiling is on.
+struct StageScope {
+    int stage;
+    cudaStream_t s;
+    cudaEvent_t a = nullptr;
+    StageScope(int st, cudaStream_t stream) : stage(st), s(stream)
+    {
+        g_launches.fetch_add(1, std::memory_order_relaxed);
+        std::lock_guard<std::mutex> lk(g_prof.mu);
+        if (g_prof.on) {
+            a = g_prof.ev();
+            cudaEventRecord(a, s);
+        }
+    }
+    ~StageScope()
+    {
+        if (!a) return;
+        std::lock_guard<std::mutex> lk(g_prof.mu);
+        cudaEvent_t b = g_prof.ev();
+        cudaEventRecord(b, s);
+        g_prof.recs.push_back({stage, a, b});
+    }
+};
+
 bool valid_bandwidth(int B) { return B >= 1 && B <= kMaxBandwidth; }
 
 size_t grid_elems(int B)
@@ -98,7 +153,10 @@ int get_tables(int B, cudaStream_t stream, BandTables* out)
     cudaError_t e = cudaMalloc(&mem, tables_bytes(B));
     if (e != cudaSuccess) return fail(PFSOFT_ENOMEM, std::string("table allocation: ") + cudaGetErrorString(e));
     BandTables t;
-    e = tables_build(B, mem, &t, stream);
+    {
+        StageScope sc(ST_TABLES, stream);
+        e = tables_build(B, mem, &t, stream);
+    }
     if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
     if (e != cudaSuccess) {
         cudaFree(mem);
@@ -156,18 +214,10 @@ DwtArgs dwt_args(const BandTables& t)
     a.cosh = t.cosh;
     a.w = t.w;
     a.normf = t.normf;
+    a.pw_sin = t.pw_sin;
+    a.pw_cos = t.pw_cos;
     a.team_warps = dwt_team_warps(t.N);
     return a;
-}
-
-int dwt_blocks(int B, int team_warps)
-{
-    const int teams_per_cta = 4 / team_warps;
-    const int need = (num_classes(B) + teams_per_cta - 1) / teams_per_cta;
-    int dev = 0, sms = 148;
-    if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    const int cap = sms * 8;
-    return need < cap ? need : cap;
 }
 
 int check_transform_args(const void* a, const void* b, int B, void*& ws, size_t ws_bytes)
@@ -197,10 +247,19 @@ int run_dsoft(const double* d_grid, int B, double* d_coeffs, void* ws, cudaStrea
     // F2: vectors = layers k, tile = gamma bin r, elements = column c; in place on X
     FftPassArgs f2 = pass_args(N, N, t, FftStrides{1, n2, n}, FftStrides{1, n2, n}, 1.0);
     if (f1.nstages == 0) return fail(PFSOFT_EINVAL, "FFT length cannot be planned");
-    PF_CUDA(fft_pass_launch(G, X, f1, N, -1, s));
-    PF_CUDA(fft_pass_launch(X, X, f2, N, -1, s));
+    {
+        StageScope sc(ST_FFT_FWD_ROWS, s);
+        PF_CUDA(fft_pass_launch(G, X, f1, N, -1, s));
+    }
+    {
+        StageScope sc(ST_FFT_FWD_COLS, s);
+        PF_CUDA(fft_pass_launch(X, X, f2, N, -1, s));
+    }
     DwtArgs a = dwt_args(t);
-    PF_CUDA(dwt_forward_launch(X, reinterpret_cast<double2*>(d_coeffs), a, dwt_blocks(B, a.team_warps), s));
+    {
+        StageScope sc(ST_DWT_FWD, s);
+        PF_CUDA(dwt_forward_launch(X, reinterpret_cast<double2*>(d_coeffs), a, 0, s));
+    }
     return PFSOFT_OK;
 }
 
@@ -213,16 +272,28 @@ int run_idsoft(const double* d_coeffs, int B, double* d_grid, void* ws, cudaStre
     const long long n = N, n2 = n * n;
     double2* X = static_cast<double2*>(ws);
     double2* G = reinterpret_cast<double2*>(d_grid);
-    PF_CUDA(zero_nyquist_launch(X, B, s));
+    {
+        StageScope sc(ST_NYQUIST, s);
+        PF_CUDA(zero_nyquist_launch(X, B, s));
+    }
     DwtArgs a = dwt_args(t);
-    PF_CUDA(dwt_inverse_launch(reinterpret_cast<const double2*>(d_coeffs), X, a, dwt_blocks(B, a.team_warps), s));
+    {
+        StageScope sc(ST_DWT_INV, s);
+        PF_CUDA(dwt_inverse_launch(reinterpret_cast<const double2*>(d_coeffs), X, a, 0, s));
+    }
     // I2: inverse DFT over alpha, in place on X
     FftPassArgs i2 = pass_args(N, N, t, FftStrides{1, n2, n}, FftStrides{1, n2, n}, 1.0);
     // I1: inverse DFT over gamma, X[r][c][k] -> G[k][c][r], scaled by 1/(4B^2) (src/fn_idsoft.cpp:289)
     FftPassArgs i1 = pass_args(N, N, t, FftStrides{1, n, n2}, FftStrides{n2, n, 1}, 1.0 / (4.0 * B * B));
     if (i1.nstages == 0) return fail(PFSOFT_EINVAL, "FFT length cannot be planned");
-    PF_CUDA(fft_pass_launch(X, X, i2, N, +1, s));
-    PF_CUDA(fft_pass_launch(X, G, i1, N, +1, s));
+    {
+        StageScope sc(ST_FFT_INV_COLS, s);
+        PF_CUDA(fft_pass_launch(X, X, i2, N, +1, s));
+    }
+    {
+        StageScope sc(ST_FFT_INV_ROWS, s);
+        PF_CUDA(fft_pass_launch(X, G, i1, N, +1, s));
+    }
     return PFSOFT_OK;
 }
 
@@ -509,5 +580,48 @@ int pfsoft_cuda_wigner_d_matrix(int B, int M, int Mp, int weighted, double* d_ou
     PF_CUDA(cudaGetLastError());
     return PFSOFT_OK;
 }
+
+long long pfsoft_launch_count(void) { return g_launches.load(); }
+
+int pfsoft_tune_dwt_case_split(int direction, int case_split)
+{
+    if (direction < 0 || direction > 1 || case_split < 0 || case_split > 2) return fail(PFSOFT_EINVAL, "bad tuning value");
+    dwt_set_case_split(direction, case_split);
+    return PFSOFT_OK;
+}
+
+int pfsoft_profile_enable(int on)
+{
+    std::lock_guard<std::mutex> lk(g_prof.mu);
+    g_prof.on = on != 0;
+    return PFSOFT_OK;
+}
+
+int pfsoft_profile_read(double* ms, long long* launches, int max_stages)
+{
+    g_last_error.clear();
+    std::lock_guard<std::mutex> lk(g_prof.mu);
+    for (auto& r : g_prof.recs) {
+        float t = 0.f;
+        cudaError_t e = cudaEventSynchronize(r.b);
+        if (e == cudaSuccess) e = cudaEventElapsedTime(&t, r.a, r.b);
+        if (e != cudaSuccess) return cuda_fail(e, "pfsoft_profile_read");
+        g_prof.ms[r.stage] += t;
+        g_prof.count[r.stage] += 1;
+        g_prof.pool.push_back(r.a);
+        g_prof.pool.push_back(r.b);
+    }
+    g_prof.recs.clear();
+    const int n = max_stages < ST_COUNT ? max_stages : ST_COUNT;
+    for (int i = 0; i < n; ++i) {
+        if (ms) ms[i] = g_prof.ms[i];
+        if (launches) launches[i] = g_prof.count[i];
+        g_prof.ms[i] = 0.0;
+        g_prof.count[i] = 0;
+    }
+    return ST_COUNT;
+}
+
+const char* pfsoft_profile_stage_name(int stage) { return (stage >= 0 && stage < ST_COUNT) ? kStageNames[stage] : ""; }
 
 }  // extern "C"

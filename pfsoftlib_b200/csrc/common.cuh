@@ -68,26 +68,40 @@ struct PairCase {
     double s0;
 };
 
-__host__ __device__ __forceinline__ int class_cases(int M, int Mp, int N, PairCase* out)
+// Number of distinct coefficients class (M, M') serves: 1 for (0,0), 4 when M' = 0 or M' = M,
+// otherwise 8.
+__host__ __device__ __forceinline__ int class_case_count(int M, int Mp)
 {
-    const int c1[8] = {M, Mp, -M, -Mp, Mp, M, -Mp, -M};
-    const int c2[8] = {Mp, M, -Mp, -M, -M, -Mp, M, Mp};
-    int n = 0;
-    for (int i = 0; i < 8; ++i) {
-        bool dup = false;
-        for (int j = 0; j < n; ++j) dup |= (out[j].m1 == c1[i] && out[j].m2 == c2[i]);
-        if (dup) continue;
-        PairCase& p = out[n++];
-        p.m1 = c1[i];
-        p.m2 = c2[i];
-        p.row = c2[i] >= 0 ? c2[i] : N + c2[i];
-        p.col = c1[i] >= 0 ? c1[i] : N + c1[i];
-        p.rev = (c1[i] < 0) != (c2[i] < 0);
-        const int a1 = c1[i] < 0 ? -c1[i] : c1[i];
-        const bool x = (a1 == M) ? (c1[i] < 0) : (c2[i] > 0);
-        p.s0 = (x && ((M - Mp) & 1)) ? 1.0 : -1.0;
+    return M == 0 ? 1 : ((Mp == 0 || Mp == M) ? 4 : 8);
+}
+
+// Case c (< class_case_count) of class (M, M'). The eight orientations, in this order, are
+//   (M,M') (M',M) (-M,-M') (-M',-M) (M',-M) (M,-M') (-M',M) (-M,M');
+// for M' = 0 the first four are distinct, for M' = M the even ones.
+__host__ __device__ __forceinline__ PairCase class_case(int M, int Mp, int c, int N)
+{
+    const int e = (Mp == M && M > 0) ? 2 * c : c;
+    int m1, m2;
+    switch (e) {
+        case 0: m1 = M; m2 = Mp; break;
+        case 1: m1 = Mp; m2 = M; break;
+        case 2: m1 = -M; m2 = -Mp; break;
+        case 3: m1 = -Mp; m2 = -M; break;
+        case 4: m1 = Mp; m2 = -M; break;
+        case 5: m1 = M; m2 = -Mp; break;
+        case 6: m1 = -Mp; m2 = M; break;
+        default: m1 = -M; m2 = Mp; break;
     }
-    return n;
+    PairCase p;
+    p.m1 = m1;
+    p.m2 = m2;
+    p.row = m2 >= 0 ? m2 : N + m2;
+    p.col = m1 >= 0 ? m1 : N + m1;
+    p.rev = (m1 < 0) != (m2 < 0);
+    const int a1 = m1 < 0 ? -m1 : m1;
+    const bool x = (a1 == M) ? (m1 < 0) : (m2 > 0);
+    p.s0 = (x && ((M - Mp) & 1)) ? 1.0 : -1.0;
+    return p;
 }
 
 }  // namespace pfsoft_dev

@@ -1,26 +1,29 @@
-// Discrete Wigner transform (DWT) over beta for every order class, FP64 on CUDA cores (sm_100a).
+// Discrete Wigner transform (DWT) over beta for every order class, FP64 (sm_100a).
 //
-// For the class (M, M'), M >= M' >= 0, one "team" of 1, 2 or 4 warps generates the reference's
-// Wigner rows d_{M,M'}(l, beta_k), l = M..B-1, on chip with the three-term recurrence in l
+// For the class (M, M'), M >= M' >= 0, one "team" of TW warps generates the reference's Wigner
+// rows d_{M,M'}(l, beta_k), l = M..B-1, on chip with the three-term recurrence in l
 // (include/PFSOFTlib_headers/fn_dwt.hpp:167-199) and applies them to the up to eight beta
 // columns the reference serves from one matrix (src/fn_dsoft.cpp:137-283,
-// src/fn_idsoft.cpp:127-283). Nothing is stored: lane `tl` of the team owns beta columns
-// k = tl + t*team_threads (t < KT), keeps d(l-1, k) and d(l, k) in registers and advances them
-// one degree per step.
+// src/fn_idsoft.cpp:127-283). The matrix is never stored: warp w of the team owns beta columns
+// [w*KW, w*KW + KW), KW = 32*KT, and lane i runs the recurrence for columns w*KW + i + 32j,
+// keeping d(l-1, k) and d(l, k) in registers. A few degrees at a time the fresh rows go to
+// shared memory and the contraction over beta runs on the FP64 MMA (mma.sync m8n8k4 f64):
 //
-//   forward  f^l_{m1,m2} = pi/(2B^2) sign(l) sum_k d(l, k) X[row][col][rev ? N-1-k : k]
-//            (weighted rows). Per degree every lane forms 16 partial sums (8 columns x re/im)
-//            over its KT betas; a 5-step butterfly transpose-reduce over the warp leaves each
-//            sum in one lane pair, multi-warp teams add their warps through shared memory.
-//   inverse  X[row][col][rev ? N-1-k : k] = sum_l d'(l, k) sign(l) (2B^2/pi) f^l_{m1,m2}
-//            (unweighted rows). The coefficients are staged in shared memory in chunks of 32
-//            degrees and broadcast; each lane accumulates its own betas, no reduction.
+//   forward  F[l][v] = sum_k D[l][k] S[k][v], S[k][v] = component (v&1) of
+//            X[row][col][rev ? N-1-k : k] for case v/2 (weighted rows, 8 degrees per MMA tile);
+//            the TW warps' partial sums over their beta ranges are added in shared memory and
+//            written as f^l = pi/(2B^2) sign(l) F[l].
+//   inverse  S[k][v] = sum_l D[l][k] G[l][v], G = (2B^2/pi) sign(l) f^l staged in shared memory
+//            in chunks of 32 degrees (prefetched one chunk ahead); 4 degrees per MMA; each warp
+//            owns its columns, so nothing is reduced across warps.
 //
 // Seeds. d(M, k) = -normf * sin(beta_k/2)^(M-M') * cos(beta_k/2)^(M+M') (* w_k) can fall far
 // below the FP64 range (the reference's x87 long double hides this). Seeds are formed with a
 // separate binary exponent; a column whose seed is below 2^-900 runs the recurrence scaled by
 // 2^(600 s) and rescales when it grows past 2^300. While s > 0 its true magnitude is below
 // 2^-300 and it contributes nothing at FP64 precision, so it is skipped.
+//
+// Scheduling: a persistent grid; classes (longest first) are dealt to teams in snake order.
 
 #include "common.cuh"
 #include "dwt.cuh"
@@ -32,28 +35,6 @@ namespace {
 constexpr int kWarps = 4;     // warps per CTA
 constexpr int kLB = 32;       // degrees per reduction / coefficient chunk
 constexpr double kPi = 3.141592653589793;
-
-// x^p as (m, e) with x^p = m 2^e, m in [0.5, 1); x > 0
-__device__ __forceinline__ void ext_pow(double x, int p, double& rm, int& re)
-{
-    int xe;
-    double xm = frexp(x, &xe);
-    rm = 1.0;
-    re = 0;
-    while (p) {
-        if (p & 1) {
-            int t;
-            rm = frexp(rm * xm, &t);
-            re += xe + t;
-        }
-        p >>= 1;
-        if (p) {
-            int t;
-            xm = frexp(xm * xm, &t);
-            xe = 2 * xe + t;
-        }
-    }
-}
 
 // Recurrence step degree l -> l+1 for orders (M, Mp) (fn_dwt.hpp:167-192):
 //   d(l+1) = c1 d(l-1) + d(l) f1 (f2 + cos beta)
@@ -76,15 +57,13 @@ __device__ __forceinline__ void rec_coef(int l, int M, int Mp, double& c1, doubl
     }
 }
 
-// Seed of one beta column with its scale count (see the header comment).
-__device__ __forceinline__ double seed_value(double nf_w, double sh, double ch, int sp, int cp, int& sc)
+// Seed of one beta column with its scale count (see the header comment): nf_w * s * c where s
+// and c are table powers {mantissa, exponent}.
+__device__ __forceinline__ double seed_value(double nf_w, double2 s, double2 c, int& sc)
 {
-    double ms, mc;
-    int es, ec, ev;
-    ext_pow(sh, sp, ms, es);
-    ext_pow(ch, cp, mc, ec);
-    const double v = frexp(nf_w * ms * mc, &ev);
-    const int E = ev + es + ec;
+    int ev;
+    const double v = frexp(nf_w * s.x * c.x, &ev);
+    const int E = ev + (int)s.y + (int)c.y;
     if (E >= -900) {
         sc = 0;
         return -ldexp(v, E);
@@ -93,53 +72,14 @@ __device__ __forceinline__ double seed_value(double nf_w, double sh, double ch, 
     return -ldexp(v, E + 600 * sc);
 }
 
-__device__ __forceinline__ void team_sync(int team, int team_warps)
+template <int TW>
+__device__ __forceinline__ void team_sync(int team)
 {
-    if (team_warps == 1) {
+    if (TW == 1) {
         __syncwarp();
     } else {
-        asm volatile("bar.sync %0, %1;" ::"r"(1 + team), "r"(32 * team_warps) : "memory");
+        asm volatile("bar.sync %0, %1;" ::"r"(1 + team), "r"(32 * TW) : "memory");
     }
-}
-
-// lane -> index of the fully reduced value it holds after warp_reduce16
-__device__ __forceinline__ int reduced_index(int lane)
-{
-    return ((lane >> 4) & 1) * 8 + ((lane >> 3) & 1) * 4 + ((lane >> 2) & 1) * 2 + ((lane >> 1) & 1);
-}
-
-// Butterfly transpose-reduce of 16 values over the 32 lanes: 16 shuffles of a double.
-__device__ __forceinline__ double warp_reduce16(double (&v)[16], int lane)
-{
-#pragma unroll
-    for (int i = 0; i < 8; ++i) {
-        const bool up = lane & 16;
-        const double send = up ? v[i] : v[i + 8];
-        const double keep = up ? v[i + 8] : v[i];
-        v[i] = keep + __shfl_xor_sync(0xffffffffu, send, 16);
-    }
-#pragma unroll
-    for (int i = 0; i < 4; ++i) {
-        const bool up = lane & 8;
-        const double send = up ? v[i] : v[i + 4];
-        const double keep = up ? v[i + 4] : v[i];
-        v[i] = keep + __shfl_xor_sync(0xffffffffu, send, 8);
-    }
-#pragma unroll
-    for (int i = 0; i < 2; ++i) {
-        const bool up = lane & 4;
-        const double send = up ? v[i] : v[i + 2];
-        const double keep = up ? v[i + 2] : v[i];
-        v[i] = keep + __shfl_xor_sync(0xffffffffu, send, 4);
-    }
-    {
-        const bool up = lane & 2;
-        const double send = up ? v[0] : v[1];
-        const double keep = up ? v[1] : v[0];
-        v[0] = keep + __shfl_xor_sync(0xffffffffu, send, 2);
-    }
-    v[0] += __shfl_xor_sync(0xffffffffu, v[0], 1);
-    return v[0];
 }
 
 __device__ __forceinline__ double case_sign(const PairCase& p, int l, int M)
@@ -147,263 +87,434 @@ __device__ __forceinline__ double case_sign(const PairCase& p, int l, int M)
     return (p.rev && ((l - M) & 1)) ? -p.s0 : p.s0;
 }
 
-template <int KT>
-__global__ void __launch_bounds__(kWarps * 32) dwt_forward_kernel(const double2* __restrict__ X,
-                                                                  double* __restrict__ out, const DwtArgs a)
+// One FP64 MMA: C(8x8) += A(8x4, row) * B(4x8, col). Fragments per lane (g = lane/4, t = lane%4):
+// A[g][t], B[t][g], C[g][2t], C[g][2t+1].
+__device__ __forceinline__ void dmma(double& c0, double& c1, double a, double b)
 {
-    __shared__ double s_rc[kWarps][kLB][3];
-    __shared__ double s_red[kWarps][kLB][16];
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int TW = a.team_warps;
-    const int team = warp / TW;
-    const int teams_per_cta = kWarps / TW;
-    const int tthreads = 32 * TW;
-    const int tl = (warp - team * TW) * 32 + lane;
+    asm("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};"
+        : "+d"(c0), "+d"(c1)
+        : "d"(a), "d"(b));
+}
+
+// Snake (boustrophedon) order over the longest-first class list: team `my` of `T` takes
+// classes r*T + my in even rounds and r*T + T-1-my in odd rounds.
+__device__ __forceinline__ int snake_class(int r, int T, int my) { return r * T + ((r & 1) ? (T - 1 - my) : my); }
+
+template <int KT>
+struct ColumnState {
+    double cb[KT], dcur[KT], dprev[KT], keep[KT];
+    int sc[KT];
+    bool scaled;
+
+    __device__ __forceinline__ void seed(const DwtArgs& a, const int* kc, double nf, bool weighted, int M, int Mp)
+    {
+        bool any = false;
+#pragma unroll
+        for (int j = 0; j < KT; ++j) {
+            const int k = kc[j];
+            dprev[j] = 0.0;
+            sc[j] = 0;
+            dcur[j] = k < a.N ? seed_value(weighted ? nf * a.w[k] : nf, a.pw_sin[(size_t)(M - Mp) * a.N + k],
+                                           a.pw_cos[(size_t)(M + Mp) * a.N + k], sc[j])
+                              : 0.0;
+            keep[j] = sc[j] ? 0.0 : 1.0;
+            any |= sc[j] > 0;
+        }
+        scaled = __any_sync(0xffffffffu, any);
+    }
+
+    // d(l) of the lane's columns into row[lane + 32j]; a column still below 2^-300 stores 0
+    __device__ __forceinline__ void store(double* row, int lane) const
+    {
+        if (!scaled) {
+#pragma unroll
+            for (int j = 0; j < KT; ++j) row[lane + 32 * j] = dcur[j];
+        } else {
+#pragma unroll
+            for (int j = 0; j < KT; ++j) row[lane + 32 * j] = dcur[j] * keep[j];
+        }
+    }
+
+    // d(l+1) = c1 d(l-1) + d(l) (a + b cos beta), with a = f1 f2 and b = f1
+    __device__ __forceinline__ void advance(double c1, double a, double b)
+    {
+#pragma unroll
+        for (int j = 0; j < KT; ++j) {
+            const double t = fma(b, cb[j], a);
+            const double nx = fma(c1, dprev[j], dcur[j] * t);
+            dprev[j] = dcur[j];
+            dcur[j] = nx;
+        }
+        if (scaled) {
+            bool still = false;
+#pragma unroll
+            for (int j = 0; j < KT; ++j) {
+                if (sc[j] && fabs(dcur[j]) >= 0x1p300) {
+                    dcur[j] *= 0x1p-600;
+                    dprev[j] *= 0x1p-600;
+                    if (--sc[j] == 0) keep[j] = 1.0;
+                }
+                still |= sc[j] > 0;
+            }
+            scaled = __any_sync(0xffffffffu, still);
+        }
+    }
+};
+
+template <int KT>
+struct FwdSmem {
+    static constexpr int KW = 32 * KT;
+    static constexpr int DS = KW + 4;   // padded row stride: A-fragment loads hit distinct banks
+    static constexpr size_t d_off = 0;                                       // [kWarps][2][8][DS]
+    static constexpr size_t rc_off = d_off + (size_t)kWarps * 2 * 8 * DS;     // [kWarps][kLB][4]
+    static constexpr size_t red_off = rc_off + (size_t)kWarps * kLB * 4;     // [2][kWarps][8][16]
+    static constexpr size_t doubles = red_off + (size_t)2 * kWarps * 8 * 16;
+};
+
+template <int KT>
+struct InvSmem {
+    static constexpr int KW = 32 * KT;
+    static constexpr int DS = KW + 8;   // padded row stride for the transposed A-fragment loads
+    static constexpr size_t d_off = 0;                                       // [kWarps][2][4][DS]
+    static constexpr size_t rc_off = d_off + (size_t)kWarps * 2 * 4 * DS;     // [kWarps][kLB][4]
+    static constexpr size_t g_off = rc_off + (size_t)kWarps * kLB * 4;       // [teams][2][kLB][16]
+    static constexpr size_t doubles = g_off + (size_t)kWarps * 2 * kLB * 16;
+};
+
+// Recurrence coefficients for degrees l .. l+31 of one warp: rc[i] = {c1, f1 f2, f1, -} for the
+// step l+i -> l+i+1 (one lane per degree). Steps past the last degree are filled as well (their
+// values stay finite and only feed rows that are never used), so the step loop has no guards.
+__device__ __forceinline__ void fill_rc4(double* rc, int l, int M, int Mp, int lane)
+{
+    __syncwarp();
+    double c1, f1, f2;
+    rec_coef(l + lane, M, Mp, c1, f1, f2);
+    *reinterpret_cast<double2*>(rc + 4 * lane) = make_double2(c1, f1 * f2);
+    rc[4 * lane + 2] = f1;
+    __syncwarp();
+}
+
+// One recurrence step: store d(l) into `row`, advance to d(l+1).
+template <int KT>
+__device__ __forceinline__ void gen_step(ColumnState<KT>& cs, double* row, int lane, const double* rc)
+{
+    cs.store(row, lane);
+    const double2 ca = *reinterpret_cast<const double2*>(rc);
+    cs.advance(ca.x, ca.y, rc[2]);
+}
+
+// Team layout shared by both directions: TW column warps x CS case warps. Warp `wt` of the team
+// owns beta columns [cw*KW, cw*KW + KW) (cw = wt / CS) and, with CS = 2, only the four cases
+// 4h .. 4h+3 (h = wt % CS, one MMA n-tile); the pair of case warps runs the same recurrence
+// (FP64 pipe) so that each holds half of the MMA operands (tensor pipe) in registers.
+template <int KT, int TW, int CS>
+struct Team {
+    static constexpr int WARPS = TW * CS;
+    static constexpr int PER_CTA = kWarps / WARPS;
+    static constexpr int NT = 2 / CS;   // MMA n-tiles (groups of 4 cases) per warp
+    int warp, lane, g, t4, team, wt, cw, h, tl;
+    __device__ __forceinline__ Team()
+    {
+        warp = threadIdx.x >> 5;
+        lane = threadIdx.x & 31;
+        g = lane >> 2;
+        t4 = lane & 3;
+        team = warp / WARPS;
+        wt = warp - team * WARPS;
+        cw = wt / CS;
+        h = wt - cw * CS;
+        tl = wt * 32 + lane;
+    }
+};
+
+// Forward DWT (see the header comment). The rows of 8-degree block b+1 are generated while
+// block b is contracted (two row buffers).
+template <int KT, int TW, int CS>
+__global__ void __launch_bounds__(kWarps * 32, CS == 2 ? 4 : 1)
+    dwt_forward_kernel(const double2* __restrict__ X, double* __restrict__ out, const DwtArgs a)
+{
+    using L = FwdSmem<KT>;
+    using TM = Team<KT, TW, CS>;
+    constexpr int KW = L::KW, DS = L::DS, NSUB = KW / 4, QPS = NSUB / 8;   // subtiles per step
+    constexpr int NT = TM::NT;
+    extern __shared__ double smem[];
+    const TM tm;
+    const int lane = tm.lane, g = tm.g, t4 = tm.t4;
+    double* s_d = smem + L::d_off + (size_t)tm.warp * 2 * 8 * DS;
+    double* s_rc = smem + L::rc_off + (size_t)tm.warp * kLB * 4;
+    double* s_red = smem + L::red_off;   // [2][warp][8][16]
     const int B = a.B, N = a.N;
     const int ncls = num_classes(B);
     const double norm = kPi / (double)(B * 2 * B);   // src/fn_dsoft.cpp:119
 
-    int kcol[KT];
-    double cb[KT];
+    int kc[KT];
+    ColumnState<KT> cs;
 #pragma unroll
-    for (int t = 0; t < KT; ++t) {
-        kcol[t] = tl + t * tthreads;
-        cb[t] = kcol[t] < N ? a.cosb[kcol[t]] : 0.0;
+    for (int j = 0; j < KT; ++j) {
+        kc[j] = tm.cw * KW + lane + 32 * j;
+        cs.cb[j] = kc[j] < N ? a.cosb[kc[j]] : 0.0;
     }
 
-    for (int cls = blockIdx.x * teams_per_cta + team; cls < ncls; cls += gridDim.x * teams_per_cta) {
+    const int T = gridDim.x * TM::PER_CTA;
+    const int my = blockIdx.x * TM::PER_CTA + tm.team;
+    int redbuf = 0;
+    for (int r = 0;; ++r) {
+        const int cls = snake_class(r, T, my);
+        if (cls >= ncls) break;
         int M, Mp;
         class_orders(cls, M, Mp);
-        PairCase pc[8];
-        const int nc = class_cases(M, Mp, N, pc);
+        const int nc = class_case_count(M, Mp);
 
-        double2 s[8][KT];
+        // B fragments: S[k][v] for k = cw*KW + 4q + t4 and v = 2*case + (re, im), case = 4n + g/2
+        // for this warp's n-tiles n
+        double sb[NT][NSUB];
+        PairCase po[NT];   // output cases 4n + t4 held by this lane
 #pragma unroll
-        for (int c = 0; c < 8; ++c) {
-            const double2* col = X + ((size_t)pc[c < nc ? c : 0].row * N + pc[c < nc ? c : 0].col) * N;
-            const bool rev = pc[c < nc ? c : 0].rev;
+        for (int n = 0; n < NT; ++n) {
+            const int nn = CS == 2 ? tm.h : n;
+            const int c = 4 * nn + (g >> 1), comp = g & 1;
+            const bool ok = c < nc;
+            const PairCase p = class_case(M, Mp, ok ? c : 0, N);
+            const double* col = reinterpret_cast<const double*>(X + ((size_t)p.row * N + p.col) * N) + comp;
 #pragma unroll
-            for (int t = 0; t < KT; ++t) {
-                const int k = kcol[t];
-                s[c][t] = (c < nc && k < N) ? __ldg(col + (rev ? N - 1 - k : k)) : make_double2(0.0, 0.0);
+            for (int q = 0; q < NSUB; ++q) {
+                const int k = tm.cw * KW + 4 * q + t4;
+                sb[n][q] = (ok && k < N) ? __ldg(col + 2 * (p.rev ? N - 1 - k : k)) : 0.0;
             }
+            po[n] = class_case(M, Mp, 4 * nn + t4 < nc ? 4 * nn + t4 : 0, N);
         }
 
-        const double nf = a.normf[cls];
-        double dcur[KT], dprev[KT];
-        int sc[KT];
-        bool any = false;
+        cs.seed(a, kc, a.normf[cls], true, M, Mp);
+        fill_rc4(s_rc, M, M, Mp, lane);
 #pragma unroll
-        for (int t = 0; t < KT; ++t) {
-            const int k = kcol[t];
-            dprev[t] = 0.0;
-            sc[t] = 0;
-            dcur[t] = k < N ? seed_value(nf * a.w[k], a.sinh[k], a.cosh[k], M - Mp, M + Mp, sc[t]) : 0.0;
-            any |= sc[t] > 0;
-        }
-        bool scaled = __any_sync(0xffffffffu, any);
-
-        const int myv = reduced_index(lane);
-        const int myc = myv >> 1;
-        for (int l = M; l < B; ++l) {
-            const int li = l - M;
-            const int slot = li & (kLB - 1);
-            if (slot == 0) {
-                __syncwarp();
-                const int ll = l + lane;
-                if (ll < B - 1) {
-                    double c1, f1, f2;
-                    rec_coef(ll, M, Mp, c1, f1, f2);
-                    s_rc[warp][lane][0] = c1;
-                    s_rc[warp][lane][1] = f1;
-                    s_rc[warp][lane][2] = f2;
+        for (int s = 0; s < 8; ++s) gen_step<KT>(cs, s_d + s * DS, lane, s_rc + 4 * s);   // block 0
+        __syncwarp();
+        const int nblk = (B - M + 7) >> 3;
+        int cur = 0;
+        for (int blk = 0; blk < nblk; ++blk) {
+            const int l0 = M + 8 * blk;
+            const double* dc = s_d + cur * 8 * DS;
+            double* dn = s_d + (cur ^ 1) * 8 * DS;
+            double acc[2][NT][2];
+#pragma unroll
+            for (int e = 0; e < 2; ++e)
+#pragma unroll
+                for (int n = 0; n < NT; ++n) acc[e][n][0] = acc[e][n][1] = 0.0;
+            auto mma_step = [&](int s) {
+#pragma unroll
+                for (int i = 0; i < QPS; ++i) {
+                    const int q = s * QPS + i;
+                    const double av = dc[g * DS + 4 * q + t4];
+#pragma unroll
+                    for (int n = 0; n < NT; ++n) dmma(acc[q & 1][n][0], acc[q & 1][n][1], av, sb[n][q]);
                 }
-                __syncwarp();
-            }
-            double acc[16];
+            };
+            if (blk + 1 < nblk) {
+                // contract block blk while generating block blk+1 (degrees beyond B - 1 are
+                // generated too; their rows only reach outputs that are never stored)
+                const int off = 8 * (blk + 1);
+                if ((off & (kLB - 1)) == 0) fill_rc4(s_rc, M + off, M, Mp, lane);
+                const double* rcb = s_rc + 4 * (off & (kLB - 1));
 #pragma unroll
-            for (int i = 0; i < 16; ++i) acc[i] = 0.0;
-#pragma unroll
-            for (int t = 0; t < KT; ++t) {
-                const double d = (scaled && sc[t]) ? 0.0 : dcur[t];
-#pragma unroll
-                for (int c = 0; c < 8; ++c) {
-                    acc[2 * c] = fma(d, s[c][t].x, acc[2 * c]);
-                    acc[2 * c + 1] = fma(d, s[c][t].y, acc[2 * c + 1]);
-                }
-            }
-            const double val = warp_reduce16(acc, lane);
-            if (TW == 1) {
-                if (!(lane & 1) && myc < nc) {
-                    const PairCase& p = pc[myc];
-                    out[2 * coef_index(l, p.m1, p.m2) + (myv & 1)] = norm * case_sign(p, l, M) * val;
+                for (int s = 0; s < 8; ++s) {
+                    mma_step(s);
+                    gen_step<KT>(cs, dn + s * DS, lane, rcb + 4 * s);
                 }
             } else {
-                if (!(lane & 1)) s_red[warp][slot][myv] = val;
-                if (slot == kLB - 1 || l == B - 1) {
-                    team_sync(team, TW);
-                    const int l0 = l - slot;
-                    const int cnt = (slot + 1) * 16;
-                    for (int e = tl; e < cnt; e += tthreads) {
-                        const int lj = e >> 4, v = e & 15, c = v >> 1;
-                        if (c < nc) {
-                            double sum = 0.0;
-                            for (int w = 0; w < TW; ++w) sum += s_red[team * TW + w][lj][v];
-                            const PairCase& p = pc[c];
-                            const int ld = l0 + lj;
-                            out[2 * coef_index(ld, p.m1, p.m2) + (v & 1)] = norm * case_sign(p, ld, M) * sum;
-                        }
-                    }
-                    team_sync(team, TW);
-                }
-            }
-            if (l + 1 < B) {
-                const double c1 = s_rc[warp][slot][0], f1 = s_rc[warp][slot][1], f2 = s_rc[warp][slot][2];
 #pragma unroll
-                for (int t = 0; t < KT; ++t) {
-                    const double nx = fma(c1, dprev[t], (dcur[t] * f1) * (f2 + cb[t]));
-                    dprev[t] = dcur[t];
-                    dcur[t] = nx;
-                }
-                if (scaled) {
-                    bool still = false;
-#pragma unroll
-                    for (int t = 0; t < KT; ++t) {
-                        if (sc[t] && fabs(dcur[t]) >= 0x1p300) {
-                            dcur[t] *= 0x1p-600;
-                            dprev[t] *= 0x1p-600;
-                            --sc[t];
-                        }
-                        still |= sc[t] > 0;
-                    }
-                    scaled = __any_sync(0xffffffffu, still);
-                }
+                for (int s = 0; s < 8; ++s) mma_step(s);
             }
+            // lane holds the partial F[l0+g][case 4n + t4] = (r[n][0], r[n][1])
+            double rr[NT][2];
+#pragma unroll
+            for (int n = 0; n < NT; ++n) {
+                rr[n][0] = acc[0][n][0] + acc[1][n][0];
+                rr[n][1] = acc[0][n][1] + acc[1][n][1];
+            }
+            if (TW == 1) {
+                const int l = l0 + g;
+#pragma unroll
+                for (int n = 0; n < NT; ++n) {
+                    const int c = 4 * (CS == 2 ? tm.h : n) + t4;
+                    if (l < B && c < nc) {
+                        const double f = norm * case_sign(po[n], l, M);
+                        *reinterpret_cast<double2*>(out + 2 * coef_index(l, po[n].m1, po[n].m2)) =
+                            make_double2(f * rr[n][0], f * rr[n][1]);
+                    }
+                }
+            } else {
+                // partial sums of the column warps meet in a double-buffered slot: the buffer
+                // written here was last read before the previous team barrier
+                double* red = s_red + ((size_t)redbuf * kWarps + tm.warp) * 128 + g * 16;
+#pragma unroll
+                for (int n = 0; n < NT; ++n)
+                    *reinterpret_cast<double2*>(red + 8 * (CS == 2 ? 0 : n) + 2 * t4) = make_double2(rr[n][0], rr[n][1]);
+                team_sync<TM::WARPS>(tm.team);
+                for (int e = tm.tl; e < 64; e += 32 * TM::WARPS) {
+                    const int gg = e >> 3, c = e & 7;
+                    const int l = l0 + gg;
+                    if (c < nc && l < B) {
+                        // case c lives in n-tile c/4: slot (c%4) of warp (cw, h = c/4) when CS = 2
+                        double2 sum = make_double2(0.0, 0.0);
+#pragma unroll
+                        for (int w = 0; w < TW; ++w) {
+                            const int wsrc = tm.team * TM::WARPS + w * CS + (CS == 2 ? (c >> 2) : 0);
+                            const int slot = CS == 2 ? 2 * (c & 3) : 2 * c;
+                            const double2 v = *reinterpret_cast<const double2*>(
+                                s_red + ((size_t)redbuf * kWarps + wsrc) * 128 + gg * 16 + slot);
+                            sum.x += v.x;
+                            sum.y += v.y;
+                        }
+                        const PairCase p = class_case(M, Mp, c, N);
+                        const double f = norm * case_sign(p, l, M);
+                        *reinterpret_cast<double2*>(out + 2 * coef_index(l, p.m1, p.m2)) = make_double2(f * sum.x, f * sum.y);
+                    }
+                }
+                redbuf ^= 1;
+            }
+            __syncwarp();
+            cur ^= 1;
         }
-        __syncwarp();
     }
 }
 
-template <int KT>
-__global__ void __launch_bounds__(kWarps * 32) dwt_inverse_kernel(const double2* __restrict__ coeffs,
-                                                                  double2* __restrict__ X, const DwtArgs a)
+// Inverse DWT (see the header comment). Each lane ends with case 4n + t4 of its n-tiles at
+// columns cw*KW + 8p + g. The rows of 4-degree block b+1 are generated while block b is applied.
+template <int KT, int TW, int CS>
+__global__ void __launch_bounds__(kWarps * 32, CS == 2 ? 3 : 1)
+    dwt_inverse_kernel(const double2* __restrict__ coeffs, double2* __restrict__ X, const DwtArgs a)
 {
-    __shared__ double s_rc[kWarps][kLB][3];
-    __shared__ double2 s_g[kWarps][8][kLB];
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int TW = a.team_warps;
-    const int team = warp / TW;
-    const int teams_per_cta = kWarps / TW;
-    const int tthreads = 32 * TW;
-    const int tl = (warp - team * TW) * 32 + lane;
+    using L = InvSmem<KT>;
+    using TM = Team<KT, TW, CS>;
+    constexpr int KW = L::KW, DS = L::DS, NSUB8 = KW / 8, PPS = NSUB8 / 4;   // subtiles per step
+    constexpr int NT = TM::NT;
+    constexpr int TT = 32 * TM::WARPS;           // team threads
+    constexpr int PER = (8 * kLB + TT - 1) / TT; // coefficients fetched per thread per chunk
+    extern __shared__ double smem[];
+    const TM tm;
+    const int lane = tm.lane, g = tm.g, t4 = tm.t4;
+    double* s_d = smem + L::d_off + (size_t)tm.warp * 2 * 4 * DS;
+    double* s_rc = smem + L::rc_off + (size_t)tm.warp * kLB * 4;
+    double* s_g = smem + L::g_off + (size_t)tm.team * 2 * kLB * 16;   // [2][kLB][16]
     const int B = a.B, N = a.N;
     const int ncls = num_classes(B);
     const double norm = (double)(B * 2 * B) / kPi;   // src/fn_idsoft.cpp:109
 
-    int kcol[KT];
-    double cb[KT];
+    int kc[KT];
+    ColumnState<KT> cs;
 #pragma unroll
-    for (int t = 0; t < KT; ++t) {
-        kcol[t] = tl + t * tthreads;
-        cb[t] = kcol[t] < N ? a.cosb[kcol[t]] : 0.0;
+    for (int j = 0; j < KT; ++j) {
+        kc[j] = tm.cw * KW + lane + 32 * j;
+        cs.cb[j] = kc[j] < N ? a.cosb[kc[j]] : 0.0;
     }
 
-    for (int cls = blockIdx.x * teams_per_cta + team; cls < ncls; cls += gridDim.x * teams_per_cta) {
+    const int T = gridDim.x * TM::PER_CTA;
+    const int my = blockIdx.x * TM::PER_CTA + tm.team;
+    for (int r = 0;; ++r) {
+        const int cls = snake_class(r, T, my);
+        if (cls >= ncls) break;
         int M, Mp;
         class_orders(cls, M, Mp);
-        PairCase pc[8];
-        const int nc = class_cases(M, Mp, N, pc);
+        const int nc = class_case_count(M, Mp);
 
-        const double nf = a.normf[cls];
-        double dcur[KT], dprev[KT];
-        int sc[KT];
-        bool any = false;
+        // coefficients of degrees l .. l+31, scaled and signed, fetched into registers
+        double2 pf[PER];
+        auto fetch = [&](int l) {
 #pragma unroll
-        for (int t = 0; t < KT; ++t) {
-            const int k = kcol[t];
-            dprev[t] = 0.0;
-            sc[t] = 0;
-            dcur[t] = k < N ? seed_value(nf, a.sinh[k], a.cosh[k], M - Mp, M + Mp, sc[t]) : 0.0;
-            any |= sc[t] > 0;
+            for (int i = 0; i < PER; ++i) {
+                const int e = tm.tl + i * TT, c = e / kLB, ld = l + (e - c * kLB);
+                double2 v = make_double2(0.0, 0.0);
+                if (e < 8 * kLB && c < nc && ld < B) {
+                    const PairCase p = class_case(M, Mp, c, N);
+                    const double f = norm * case_sign(p, ld, M);
+                    const double2 x = __ldg(coeffs + coef_index(ld, p.m1, p.m2));
+                    v = make_double2(f * x.x, f * x.y);
+                }
+                pf[i] = v;
+            }
+        };
+        auto stash = [&](int buf) {
+#pragma unroll
+            for (int i = 0; i < PER; ++i) {
+                const int e = tm.tl + i * TT, c = e / kLB, j = e - c * kLB;
+                if (e < 8 * kLB) *reinterpret_cast<double2*>(s_g + (buf * kLB + j) * 16 + 2 * c) = pf[i];
+            }
+        };
+
+        double acc[NSUB8][NT][2];
+#pragma unroll
+        for (int p = 0; p < NSUB8; ++p)
+#pragma unroll
+            for (int n = 0; n < NT; ++n) acc[p][n][0] = acc[p][n][1] = 0.0;
+
+        fetch(M);
+        cs.seed(a, kc, a.normf[cls], false, M, Mp);
+        team_sync<TM::WARPS>(tm.team);   // the previous class is done with s_g
+        stash(0);
+        fill_rc4(s_rc, M, M, Mp, lane);
+#pragma unroll
+        for (int s = 0; s < 4; ++s) gen_step<KT>(cs, s_d + s * DS, lane, s_rc + 4 * s);   // block 0
+        team_sync<TM::WARPS>(tm.team);   // chunk 0 and block 0 rows visible
+        if (M + kLB < B) fetch(M + kLB);
+        const int nblk = (B - M + 3) >> 2;
+        int cur = 0;
+        for (int blk = 0; blk < nblk; ++blk) {
+            const int off = 4 * blk;
+            const double* dc = s_d + cur * 4 * DS;
+            double* dn = s_d + (cur ^ 1) * 4 * DS;
+            // B fragments: G[l0 + t4][v] of this warp's n-tiles (zero beyond the last degree)
+            const double* gb = s_g + ((((off >> 5) & 1) * kLB) + (off & (kLB - 1)) + t4) * 16;
+            double bv[NT];
+#pragma unroll
+            for (int n = 0; n < NT; ++n) bv[n] = gb[8 * (CS == 2 ? tm.h : n) + g];
+            auto mma_step = [&](int s) {
+#pragma unroll
+                for (int i = 0; i < PPS; ++i) {
+                    const int p = s * PPS + i;
+                    const double av = dc[t4 * DS + 8 * p + g];
+#pragma unroll
+                    for (int n = 0; n < NT; ++n) dmma(acc[p][n][0], acc[p][n][1], av, bv[n]);
+                }
+            };
+            if (blk + 1 < nblk) {
+                const int offn = off + 4;
+                const bool boundary = (offn & (kLB - 1)) == 0;
+                if (boundary) {
+                    // publish the prefetched chunk (its buffer was last read two chunks ago)
+                    stash((offn >> 5) & 1);
+                    fill_rc4(s_rc, M + offn, M, Mp, lane);
+                }
+                const double* rcb = s_rc + 4 * (offn & (kLB - 1));
+#pragma unroll
+                for (int s = 0; s < 4; ++s) {
+                    mma_step(s);
+                    gen_step<KT>(cs, dn + s * DS, lane, rcb + 4 * s);
+                }
+                if (boundary) {
+                    team_sync<TM::WARPS>(tm.team);   // new chunk visible; the old one no longer read
+                    if (M + offn + kLB < B) fetch(M + offn + kLB);
+                } else {
+                    __syncwarp();
+                }
+            } else {
+#pragma unroll
+                for (int s = 0; s < 4; ++s) mma_step(s);
+            }
+            cur ^= 1;
         }
-        bool scaled = __any_sync(0xffffffffu, any);
-
-        double2 acc[8][KT];
 #pragma unroll
-        for (int c = 0; c < 8; ++c)
-#pragma unroll
-            for (int t = 0; t < KT; ++t) acc[c][t] = make_double2(0.0, 0.0);
-
-        for (int l = M; l < B; ++l) {
-            const int slot = (l - M) & (kLB - 1);
-            if (slot == 0) {
-                team_sync(team, TW);   // the previous chunk is consumed by every warp of the team
-                for (int e = tl; e < 8 * kLB; e += tthreads) {
-                    const int c = e / kLB, j = e - c * kLB, ld = l + j;
-                    double2 g = make_double2(0.0, 0.0);
-                    if (c < nc && ld < B) {
-                        const PairCase& p = pc[c];
-                        const double f = norm * case_sign(p, ld, M);
-                        const double2 x = __ldg(coeffs + coef_index(ld, p.m1, p.m2));
-                        g = make_double2(f * x.x, f * x.y);
-                    }
-                    s_g[team][c][j] = g;
-                }
-                const int ll = l + lane;
-                if (ll < B - 1) {
-                    double c1, f1, f2;
-                    rec_coef(ll, M, Mp, c1, f1, f2);
-                    s_rc[warp][lane][0] = c1;
-                    s_rc[warp][lane][1] = f1;
-                    s_rc[warp][lane][2] = f2;
-                }
-                team_sync(team, TW);
-            }
-#pragma unroll
-            for (int c = 0; c < 8; ++c) {
-                const double2 g = s_g[team][c][slot];
-#pragma unroll
-                for (int t = 0; t < KT; ++t) {
-                    const double d = (scaled && sc[t]) ? 0.0 : dcur[t];
-                    acc[c][t].x = fma(d, g.x, acc[c][t].x);
-                    acc[c][t].y = fma(d, g.y, acc[c][t].y);
-                }
-            }
-            if (l + 1 < B) {
-                const double c1 = s_rc[warp][slot][0], f1 = s_rc[warp][slot][1], f2 = s_rc[warp][slot][2];
-#pragma unroll
-                for (int t = 0; t < KT; ++t) {
-                    const double nx = fma(c1, dprev[t], (dcur[t] * f1) * (f2 + cb[t]));
-                    dprev[t] = dcur[t];
-                    dcur[t] = nx;
-                }
-                if (scaled) {
-                    bool still = false;
-#pragma unroll
-                    for (int t = 0; t < KT; ++t) {
-                        if (sc[t] && fabs(dcur[t]) >= 0x1p300) {
-                            dcur[t] *= 0x1p-600;
-                            dprev[t] *= 0x1p-600;
-                            --sc[t];
-                        }
-                        still |= sc[t] > 0;
-                    }
-                    scaled = __any_sync(0xffffffffu, still);
-                }
-            }
-        }
-#pragma unroll
-        for (int c = 0; c < 8; ++c) {
+        for (int n = 0; n < NT; ++n) {
+            const int c = 4 * (CS == 2 ? tm.h : n) + t4;
             if (c < nc) {
-                double2* col = X + ((size_t)pc[c].row * N + pc[c].col) * N;
+                const PairCase pcase = class_case(M, Mp, c, N);
+                double2* col = X + ((size_t)pcase.row * N + pcase.col) * N;
 #pragma unroll
-                for (int t = 0; t < KT; ++t) {
-                    const int k = kcol[t];
-                    if (k < N) col[pc[c].rev ? N - 1 - k : k] = acc[c][t];
+                for (int p = 0; p < NSUB8; ++p) {
+                    const int k = tm.cw * KW + 8 * p + g;
+                    if (k < N) col[pcase.rev ? N - 1 - k : k] = make_double2(acc[p][n][0], acc[p][n][1]);
                 }
             }
         }
-        team_sync(team, TW);   // s_g / s_rc reuse by the next class
     }
 }
 
@@ -427,21 +538,40 @@ __global__ void zero_nyquist_kernel(double2* X, int B)
     }
 }
 
-template <int KT>
+// Resident CTAs on all SMs (the persistent grid).
+template <typename K>
+int persistent_blocks(K kernel, size_t smem)
+{
+    int dev = 0, sms = 148, per = 1;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kernel, kWarps * 32, smem) != cudaSuccess || per < 1) per = 1;
+    return sms * per;
+}
+
+template <int KT, int TW, int CS>
 cudaError_t launch_fwd(const double2* X, double2* coeffs, const DwtArgs& a, int nblocks, cudaStream_t s)
 {
-    dwt_forward_kernel<KT><<<nblocks, kWarps * 32, 0, s>>>(X, reinterpret_cast<double*>(coeffs), a);
+    const size_t smem = FwdSmem<KT>::doubles * sizeof(double);
+    auto k = dwt_forward_kernel<KT, TW, CS>;
+    cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    if (nblocks <= 0) nblocks = persistent_blocks(k, smem);
+    k<<<nblocks, kWarps * 32, smem, s>>>(X, reinterpret_cast<double*>(coeffs), a);
     return cudaGetLastError();
 }
 
-template <int KT>
+template <int KT, int TW, int CS>
 cudaError_t launch_inv(const double2* coeffs, double2* X, const DwtArgs& a, int nblocks, cudaStream_t s)
 {
-    dwt_inverse_kernel<KT><<<nblocks, kWarps * 32, 0, s>>>(coeffs, X, a);
+    const size_t smem = InvSmem<KT>::doubles * sizeof(double);
+    auto k = dwt_inverse_kernel<KT, TW, CS>;
+    cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    if (nblocks <= 0) nblocks = persistent_blocks(k, smem);
+    k<<<nblocks, kWarps * 32, smem, s>>>(coeffs, X, a);
     return cudaGetLastError();
 }
-
-int cols_per_lane(const DwtArgs& a) { return (a.N + 32 * a.team_warps - 1) / (32 * a.team_warps); }
 
 }  // namespace
 
@@ -452,24 +582,38 @@ int dwt_team_warps(int N)
     return 4;
 }
 
+// Team shapes by beta-column count N = 2B: KT columns per lane, TW column warps, CS case warps
+// (CS = 2 splits the eight cases over two warps that share the recurrence). g_case_split[dir]
+// overrides CS for N > 64 (0 = default), as chosen by the autotuner.
+int g_case_split[2] = {0, 0};
+
 cudaError_t dwt_forward_launch(const double2* X, double2* coeffs, const DwtArgs& a, int nblocks, cudaStream_t s)
 {
-    const int kt = cols_per_lane(a);
-    if (kt <= 1) return launch_fwd<1>(X, coeffs, a, nblocks, s);
-    if (kt <= 2) return launch_fwd<2>(X, coeffs, a, nblocks, s);
-    if (kt <= 4) return launch_fwd<4>(X, coeffs, a, nblocks, s);
-    if (kt <= 8) return launch_fwd<8>(X, coeffs, a, nblocks, s);
+    const int N = a.N;
+    const bool split = g_case_split[0] == 2;
+    if (N <= 32) return launch_fwd<1, 1, 1>(X, coeffs, a, nblocks, s);
+    if (N <= 64) return launch_fwd<2, 1, 1>(X, coeffs, a, nblocks, s);
+    if (N <= 128) return split ? launch_fwd<4, 1, 2>(X, coeffs, a, nblocks, s) : launch_fwd<4, 1, 1>(X, coeffs, a, nblocks, s);
+    if (N <= 256) return split ? launch_fwd<4, 2, 2>(X, coeffs, a, nblocks, s) : launch_fwd<4, 2, 1>(X, coeffs, a, nblocks, s);
+    if (N <= 512) return split ? launch_fwd<8, 2, 2>(X, coeffs, a, nblocks, s) : launch_fwd<4, 4, 1>(X, coeffs, a, nblocks, s);
     return cudaErrorInvalidValue;
 }
 
 cudaError_t dwt_inverse_launch(const double2* coeffs, double2* X, const DwtArgs& a, int nblocks, cudaStream_t s)
 {
-    const int kt = cols_per_lane(a);
-    if (kt <= 1) return launch_inv<1>(coeffs, X, a, nblocks, s);
-    if (kt <= 2) return launch_inv<2>(coeffs, X, a, nblocks, s);
-    if (kt <= 4) return launch_inv<4>(coeffs, X, a, nblocks, s);
-    if (kt <= 8) return launch_inv<8>(coeffs, X, a, nblocks, s);
+    const int N = a.N;
+    const bool split = g_case_split[1] == 2;
+    if (N <= 32) return launch_inv<1, 1, 1>(coeffs, X, a, nblocks, s);
+    if (N <= 64) return launch_inv<2, 1, 1>(coeffs, X, a, nblocks, s);
+    if (N <= 128) return split ? launch_inv<4, 1, 2>(coeffs, X, a, nblocks, s) : launch_inv<4, 1, 1>(coeffs, X, a, nblocks, s);
+    if (N <= 256) return split ? launch_inv<4, 2, 2>(coeffs, X, a, nblocks, s) : launch_inv<4, 2, 1>(coeffs, X, a, nblocks, s);
+    if (N <= 512) return split ? launch_inv<8, 2, 2>(coeffs, X, a, nblocks, s) : launch_inv<4, 4, 1>(coeffs, X, a, nblocks, s);
     return cudaErrorInvalidValue;
+}
+
+void dwt_set_case_split(int dir, int cs)
+{
+    if (dir >= 0 && dir < 2) g_case_split[dir] = cs;
 }
 
 cudaError_t zero_nyquist_launch(double2* X, int B, cudaStream_t s)

@@ -15,6 +15,8 @@ struct BandTables {
     double* w = nullptr;        // quadrature weights w_B(k)      [N]   (fn_dwt.hpp:62-83)
     double* normf = nullptr;    // seed norm per order class      [B(B+1)/2] (fn_dwt.hpp:117-121)
     double2* twiddle = nullptr; // exp(-2 pi i t / N)             [N]
+    double2* pw_sin = nullptr;  // sin(beta_k/2)^p as {mantissa, exponent}  [2B][N], p < 2B
+    double2* pw_cos = nullptr;  // cos(beta_k/2)^p as {mantissa, exponent}  [2B][N]
     void* block = nullptr;      // single allocation holding all of the above
 };
 
@@ -29,9 +31,12 @@ struct DwtArgs {
     const double* cosh;
     const double* w;
     const double* normf;
+    const double2* pw_sin;
+    const double2* pw_cos;
     int team_warps;   // warps cooperating on one order class (1..4)
 };
 
+// nblocks <= 0 launches the persistent grid (all resident CTAs).
 // Forward: X (beta-innermost spectrum, N^3) -> packed coefficients, scale pi/(2B^2).
 cudaError_t dwt_forward_launch(const double2* X, double2* coeffs, const DwtArgs& a, int nblocks,
                                cudaStream_t stream);
@@ -40,6 +45,10 @@ cudaError_t dwt_inverse_launch(const double2* coeffs, double2* X, const DwtArgs&
                                cudaStream_t stream);
 // Zero the beta columns of the Nyquist bins (row == B or col == B) of X.
 cudaError_t zero_nyquist_launch(double2* X, int B, cudaStream_t stream);
+
+// Tuning: dir 0 = forward, 1 = inverse; cs 1 = all eight cases per warp, 2 = four cases per
+// warp (warp pairs share the recurrence), 0 = default.
+void dwt_set_case_split(int dir, int cs);
 
 // Team shape for a bandwidth: warps per class so that each lane owns at most 4 beta columns.
 int dwt_team_warps(int N);

@@ -180,7 +180,8 @@ __device__ __forceinline__ void run_stage_fixed(const FftPassArgs& a, int s, con
 #pragma unroll
             for (int r = 1; r < R; ++r) v[r] = cmul(v[r], twiddle(a.twiddle, r * k * step, SIGN));
         }
-        if (R == 2) dft2<SIGN>(v);
+        if (R == 1) {
+        } else if (R == 2) dft2<SIGN>(v);
         else if (R == 4) dft4<SIGN>(v[0], v[1], v[2], v[3]);
         else if (R == 8) dft8<SIGN>(v);
         else if (R == 16) dft16<SIGN>(v);
@@ -242,7 +243,7 @@ __device__ void run_stage_generic(const FftPassArgs& a, int s, const double2* gs
 }
 
 template <int SIGN>
-__global__ void __launch_bounds__(256) fft_pass_kernel(const double2* src, double2* dst,
+__global__ void __launch_bounds__(256, 2) fft_pass_kernel(const double2* src, double2* dst,
                                                        const FftPassArgs a)
 {
     extern __shared__ double2 smem[];
@@ -263,6 +264,7 @@ __global__ void __launch_bounds__(256) fft_pass_kernel(const double2* src, doubl
             case 8: run_stage_fixed<SIGN, 8>(a, s, src, dst, sin_, sout, nv, src_base, dst_base); break;
             case 4: run_stage_fixed<SIGN, 4>(a, s, src, dst, sin_, sout, nv, src_base, dst_base); break;
             case 2: run_stage_fixed<SIGN, 2>(a, s, src, dst, sin_, sout, nv, src_base, dst_base); break;
+            case 1: run_stage_fixed<SIGN, 1>(a, s, src, dst, sin_, sout, nv, src_base, dst_base); break;
             case 3: run_stage_fixed<SIGN, 3>(a, s, src, dst, sin_, sout, nv, src_base, dst_base); break;
             case 5: run_stage_fixed<SIGN, 5>(a, s, src, dst, sin_, sout, nv, src_base, dst_base); break;
             default: run_stage_generic<SIGN>(a, s, src, dst, sin_, sout, nv, src_base, dst_base); break;
@@ -283,26 +285,28 @@ int fft_plan_radices(int n, int* radix, int* ns)
         rem /= 2;
         ++p2;
     }
-    // power-of-two part in radix-16 stages, remainder folded into one or two smaller stages
-    int q = p2 / 4, rr = p2 % 4;
-    if (rr == 1 && q > 0) {
-        --q;
-        r[cnt++] = 8;
-        r[cnt++] = 4;
-    } else if (rr == 1) {
-        r[cnt++] = 2;
-    } else if (rr == 2) {
-        r[cnt++] = 4;
-    } else if (rr == 3) {
-        r[cnt++] = 8;
+    // power-of-two part: as few stages as radix 16 allows, bits spread evenly (8.8.8, 16.8)
+    if (p2 > 0) {
+        const int st = (p2 + 3) / 4;
+        for (int i = 0; i < st; ++i) {
+            const int bits = p2 / st + (i < p2 % st ? 1 : 0);
+            r[cnt++] = 1 << bits;
+        }
     }
-    for (int i = 0; i < q; ++i) r[cnt++] = 16;
     while (rem % 3 == 0) { r[cnt++] = 3; rem /= 3; }
     while (rem % 5 == 0) { r[cnt++] = 5; rem /= 5; }
     for (int p = 7; rem > 1; p += 2) {
         while (rem % p == 0) { r[cnt++] = p; rem /= p; }
     }
     if (cnt == 0) r[cnt++] = 1;
+    // A lone direct (O(R^2)) stage would read and write the same HBM vector when the pass
+    // is in place; a leading radix-1 stage (a plain copy into shared memory) separates them.
+    const bool direct = !(r[0] == 1 || r[0] == 2 || r[0] == 3 || r[0] == 4 || r[0] == 5 || r[0] == 8 || r[0] == 16);
+    if (cnt == 1 && direct) {
+        r[1] = r[0];
+        r[0] = 1;
+        cnt = 2;
+    }
     if (cnt > kFftMaxStages) return 0;
     int nsv = 1;
     for (int i = 0; i < cnt; ++i) {
@@ -322,7 +326,11 @@ size_t fft_pass_smem_bytes(const FftPassArgs& a)
 cudaError_t fft_pass_launch(const double2* src, double2* dst, const FftPassArgs& a, int ntiles, int sign,
                             cudaStream_t stream)
 {
-    const int nthreads = 256;
+    // one butterfly per thread in the widest stage, up to 256 threads
+    int widest = 1;
+    for (int s = 0; s < a.nstages; ++s) widest = a.n / a.radix[s] > widest ? a.n / a.radix[s] : widest;
+    int nthreads = ((a.kb * widest + 31) / 32) * 32;
+    if (nthreads > 256) nthreads = 256;
     dim3 grid((a.nvec + a.kb - 1) / a.kb, ntiles);
     size_t smem = fft_pass_smem_bytes(a);
     // the kernel indexes two buffers; with a single buffer the second pointer is never used

@@ -4,6 +4,9 @@
 //   w_B(j) = 2/B sin(pi(2j+1)/(4B)) sum_{k<B} sin((2j+1)(2k+1)pi/(4B))/(2k+1)   fn_dwt.hpp:62-83
 //   normf(M,M') = sqrt((2M+1)/2) prod_{i<M-M'} sqrt((2M-i)/(i+1))              fn_dwt.hpp:117-121
 //   twiddle[t] = exp(-2 pi i t/N)
+//   pw_sin[p][k], pw_cos[p][k] = sin(beta_k/2)^p, cos(beta_k/2)^p, p < 2B, as an exact binary
+//       exponent and a mantissa in [0.5, 1) (exponentiation by squaring, renormalised each
+//       product), so that Wigner seeds far below the FP64 range keep full relative precision
 // The sine arguments are reduced exactly in integers before sinpi/cospi, and the weight sum
 // is compensated (Neumaier), so each entry is within a few ulp of the exact value.
 
@@ -15,6 +18,42 @@ namespace pfsoft_dev {
 namespace {
 
 __host__ __device__ inline size_t align256(size_t x) { return (x + 255) & ~size_t(255); }
+
+// x^p as {m, e}: x^p = m 2^e, m in [0.5, 1); x > 0
+__device__ double2 ext_pow_tab(double x, int p)
+{
+    int xe;
+    double xm = frexp(x, &xe);
+    double rm = 1.0;
+    int re = 0;
+    while (p) {
+        if (p & 1) {
+            int t;
+            rm = frexp(rm * xm, &t);
+            re += xe + t;
+        }
+        p >>= 1;
+        if (p) {
+            int t;
+            xm = frexp(xm * xm, &t);
+            xe = 2 * xe + t;
+        }
+    }
+    int t;
+    rm = frexp(rm, &t);
+    return make_double2(rm, (double)(re + t));
+}
+
+__global__ void powers_kernel(int B, const double* sinh, const double* cosh, double2* pw_sin, double2* pw_cos)
+{
+    const int N = 2 * B;
+    const long long total = (long long)2 * B * N;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total; i += (long long)gridDim.x * blockDim.x) {
+        const int p = (int)(i / N), k = (int)(i - (long long)p * N);
+        pw_sin[i] = ext_pow_tab(sinh[k], p);
+        pw_cos[i] = ext_pow_tab(cosh[k], p);
+    }
+}
 
 __global__ void tables_kernel(int B, double* cosb, double* sinh, double* cosh, double* w, double* normf,
                               double2* tw)
@@ -65,7 +104,7 @@ size_t tables_bytes(int B)
 {
     const size_t N = 2 * (size_t)B;
     return 4 * align256(N * sizeof(double)) + align256(num_classes(B) * sizeof(double)) +
-           align256(N * sizeof(double2));
+           align256(N * sizeof(double2)) + 2 * align256(2 * (size_t)B * N * sizeof(double2));
 }
 
 cudaError_t tables_build(int B, void* mem, BandTables* t, cudaStream_t stream)
@@ -86,10 +125,20 @@ cudaError_t tables_build(int B, void* mem, BandTables* t, cudaStream_t stream)
     t->normf = reinterpret_cast<double*>(p);
     p += align256(num_classes(B) * sizeof(double));
     t->twiddle = reinterpret_cast<double2*>(p);
+    p += align256(N * sizeof(double2));
+    t->pw_sin = reinterpret_cast<double2*>(p);
+    p += align256(2 * (size_t)B * N * sizeof(double2));
+    t->pw_cos = reinterpret_cast<double2*>(p);
     const int threads = 128;
     int blocks = (int)((num_classes(B) + threads - 1) / threads);
     if (blocks < 1) blocks = 1;
     tables_kernel<<<blocks, threads, 0, stream>>>(B, t->cosb, t->sinh, t->cosh, t->w, t->normf, t->twiddle);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    const long long total = (long long)2 * B * N;
+    int pblocks = (int)((total + 255) / 256);
+    if (pblocks > 4096) pblocks = 4096;
+    powers_kernel<<<pblocks, 256, 0, stream>>>(B, t->sinh, t->cosh, t->pw_sin, t->pw_cos);
     return cudaGetLastError();
 }
 
