@@ -66,6 +66,17 @@ int pfsoft_cuda_dsoft(const double* d_grid, int B, double* d_coeffs, void* d_wor
 int pfsoft_cuda_idsoft(const double* d_coeffs, int B, double* d_grid, void* d_workspace,
                        size_t workspace_bytes, void* stream);
 
+/* pfsoft_cuda_dsoft_noalloc has no counterpart in the reference. It is pfsoft_cuda_dsoft for
+ * callers that cannot allocate device memory (a framework-owned, capped memory pool; a hard
+ * per-process memory limit; a loop that must not take cudaMalloc's locks or cudaFree's device
+ * synchronisation): it makes no allocation at all and uses a scratch array that the library
+ * holds in device memory from load to exit (4.25 MiB per GPU). Limit: bandwidth B <= 32; a
+ * larger B returns PFSOFT_EINVAL. The first call on a device looks up that array's device
+ * address and builds the tables for B in it; make that first call before any stream capture.
+ * All calls on a device share the array, so calls that overlap on the GPU race; nothing in it
+ * has to start at zero. Same layouts and results as pfsoft_cuda_dsoft. */
+int pfsoft_cuda_dsoft_noalloc(const double* d_grid, int B, double* d_coeffs, void* stream);
+
 /* ---- Host-resident drop-in (synchronous) ---------------------------------------------------
  * The same transforms on host buffers: copy in, transform, copy out, wait. Pinned host
  * buffers (cudaHostAlloc) make the copies asynchronous DMA; pageable ones work too.

@@ -26,6 +26,7 @@ SIGNATURES = {
     "pfsoft_workspace_bytes": (_c_size, [_c_int]),
     "pfsoft_cuda_dsoft": (_c_int, [_vp, _c_int, _vp, _vp, _c_size, _vp]),
     "pfsoft_cuda_idsoft": (_c_int, [_vp, _c_int, _vp, _vp, _c_size, _vp]),
+    "pfsoft_cuda_dsoft_noalloc": (_c_int, [_vp, _c_int, _vp, _vp]),
     "pfsoft_dsoft_host": (_c_int, [_vp, _c_int, _vp]),
     "pfsoft_idsoft_host": (_c_int, [_vp, _c_int, _vp]),
     "pfsoft_cuda_layer_wise_dft2": (_c_int, [_c_int, _c_int, _c_int, _vp, _c_double, _vp]),

@@ -167,6 +167,14 @@ int get_tables(int B, cudaStream_t stream, BandTables* out)
     return PFSOFT_OK;
 }
 
+}  // namespace
+
+namespace pfsoft_dev {
+void set_last_error(const char* msg) { g_last_error = msg; }
+}  // namespace pfsoft_dev
+
+namespace {
+
 // Library-owned workspace of at least `bytes` on the current device.
 int get_workspace(size_t bytes, void** ws)
 {

@@ -50,6 +50,9 @@ cudaError_t zero_nyquist_launch(double2* X, int B, cudaStream_t stream);
 // warp (warp pairs share the recurrence), 0 = default.
 void dwt_set_case_split(int dir, int cs);
 
+// Sets the detail string returned by pfsoft_last_error() on the calling thread.
+void set_last_error(const char* msg);
+
 // Team shape for a bandwidth: warps per class so that each lane owns at most 4 beta columns.
 int dwt_team_warps(int N);
 
