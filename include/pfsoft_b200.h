@@ -93,6 +93,10 @@ int pfsoft_idsoft_host(const double* h_coeffs, int B, double* h_grid);
  * counterpart. */
 int pfsoft_cuda_layer_wise_dft2(int cols, int rows, int lays, double* d_arr, double scale, void* stream);
 int pfsoft_cuda_layer_wise_idft2(int cols, int rows, int lays, double* d_arr, double scale, void* stream);
+/* The same on a host array (grid3D::layer_wise_DFT2/IDFT2, grid3D_cx.hpp:309-427): copy in,
+ * transform, copy out, wait. */
+int pfsoft_layer_wise_dft2_host(int cols, int rows, int lays, double* h_arr, double scale);
+int pfsoft_layer_wise_idft2_host(int cols, int rows, int lays, double* h_arr, double scale);
 
 /* ---- Discrete Wigner transform helpers ---------------------------------------------------
  * pfsoft_cuda_quadrature_weights replaces DWT::quadrature_weights

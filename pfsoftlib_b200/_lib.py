@@ -31,6 +31,8 @@ SIGNATURES = {
     "pfsoft_idsoft_host": (_c_int, [_vp, _c_int, _vp]),
     "pfsoft_cuda_layer_wise_dft2": (_c_int, [_c_int, _c_int, _c_int, _vp, _c_double, _vp]),
     "pfsoft_cuda_layer_wise_idft2": (_c_int, [_c_int, _c_int, _c_int, _vp, _c_double, _vp]),
+    "pfsoft_layer_wise_dft2_host": (_c_int, [_c_int, _c_int, _c_int, _vp, _c_double]),
+    "pfsoft_layer_wise_idft2_host": (_c_int, [_c_int, _c_int, _c_int, _vp, _c_double]),
     "pfsoft_cuda_quadrature_weights": (_c_int, [_c_int, _vp, _vp]),
     "pfsoft_cuda_wigner_d_matrix": (_c_int, [_c_int, _c_int, _c_int, _c_int, _vp, _vp]),
     "pfsoft_launch_count": (ctypes.c_longlong, []),

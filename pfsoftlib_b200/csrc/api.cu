@@ -559,6 +559,44 @@ int pfsoft_cuda_layer_wise_idft2(int cols, int rows, int lays, double* d_arr, do
     return layer_wise(cols, rows, lays, d_arr, scale, stream, +1);
 }
 
+static int layer_wise_host(int cols, int rows, int lays, double* h_arr, double scale, int sign)
+{
+    g_last_error.clear();
+    if (cols < 1 || rows < 1 || lays < 1) return fail(PFSOFT_EINVAL, "grid dimensions must be positive");
+    if (!h_arr) return fail(PFSOFT_EINVAL, "null host pointer");
+    int dev = 0;
+    PF_CUDA(cudaGetDevice(&dev));
+    DeviceState* st = device_state(dev);
+    std::lock_guard<std::mutex> lk(st->host_mu);
+    const size_t bytes = (size_t)cols * rows * lays * sizeof(double2);
+    if (!st->h_stream) PF_CUDA(cudaStreamCreateWithFlags(&st->h_stream, cudaStreamNonBlocking));
+    if (st->h_grid_bytes < bytes) {
+        if (st->h_grid) cudaFree(st->h_grid);
+        st->h_grid = nullptr;
+        st->h_grid_bytes = 0;
+        cudaError_t e = cudaMalloc(&st->h_grid, bytes);
+        if (e != cudaSuccess) return fail(PFSOFT_ENOMEM, std::string("staging allocation: ") + cudaGetErrorString(e));
+        st->h_grid_bytes = bytes;
+    }
+    cudaStream_t s = st->h_stream;
+    PF_CUDA(cudaMemcpyAsync(st->h_grid, h_arr, bytes, cudaMemcpyHostToDevice, s));
+    int rc = layer_wise(cols, rows, lays, static_cast<double*>(st->h_grid), scale, s, sign);
+    if (rc) return rc;
+    PF_CUDA(cudaMemcpyAsync(h_arr, st->h_grid, bytes, cudaMemcpyDeviceToHost, s));
+    PF_CUDA(cudaStreamSynchronize(s));
+    return PFSOFT_OK;
+}
+
+int pfsoft_layer_wise_dft2_host(int cols, int rows, int lays, double* h_arr, double scale)
+{
+    return layer_wise_host(cols, rows, lays, h_arr, scale, -1);
+}
+
+int pfsoft_layer_wise_idft2_host(int cols, int rows, int lays, double* h_arr, double scale)
+{
+    return layer_wise_host(cols, rows, lays, h_arr, scale, +1);
+}
+
 int pfsoft_cuda_quadrature_weights(int B, double* d_w, void* stream)
 {
     g_last_error.clear();

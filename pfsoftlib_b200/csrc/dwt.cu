@@ -96,6 +96,12 @@ __device__ __forceinline__ void dmma(double& c0, double& c1, double a, double b)
         : "d"(a), "d"(b));
 }
 
+// Hint: bring [p, p + bytes) into L2 (bytes a multiple of 16, p 16-byte aligned).
+__device__ __forceinline__ void prefetch_l2(const void* p, unsigned bytes)
+{
+    asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(p), "r"(bytes) : "memory");
+}
+
 // Snake (boustrophedon) order over the longest-first class list: team `my` of `T` takes
 // classes r*T + my in even rounds and r*T + T-1-my in odd rounds.
 __device__ __forceinline__ int snake_class(int r, int T, int my) { return r * T + ((r & 1) ? (T - 1 - my) : my); }
@@ -175,8 +181,8 @@ template <int KT>
 struct InvSmem {
     static constexpr int KW = 32 * KT;
     static constexpr int DS = KW + 8;   // padded row stride for the transposed A-fragment loads
-    static constexpr size_t d_off = 0;                                       // [kWarps][2][4][DS]
-    static constexpr size_t rc_off = d_off + (size_t)kWarps * 2 * 4 * DS;     // [kWarps][kLB][4]
+    static constexpr size_t d_off = 0;                                       // [kWarps][2][8][DS]
+    static constexpr size_t rc_off = d_off + (size_t)kWarps * 2 * 8 * DS;     // [kWarps][kLB][4]
     static constexpr size_t g_off = rc_off + (size_t)kWarps * kLB * 4;       // [teams][2][kLB][16]
     static constexpr size_t doubles = g_off + (size_t)kWarps * 2 * kLB * 16;
 };
@@ -284,6 +290,22 @@ __global__ void __launch_bounds__(kWarps * 32, CS == 2 ? 4 : 1)
             po[n] = class_case(M, Mp, 4 * nn + t4 < nc ? 4 * nn + t4 : 0, N);
         }
 
+        {
+            // the next class's beta columns (this warp's slice) into L2 while this one runs
+            const int nx = snake_class(r + 1, T, my);
+            if (nx < ncls && lane < 8) {
+                int M2, Mp2;
+                class_orders(nx, M2, Mp2);
+                if (lane < class_case_count(M2, Mp2)) {
+                    const PairCase p = class_case(M2, Mp2, lane, N);
+                    const int k0 = tm.cw * KW, k1 = min(N, k0 + KW);
+                    if (k0 < k1) {
+                        const int lo = p.rev ? N - k1 : k0;
+                        prefetch_l2(X + ((size_t)p.row * N + p.col) * N + lo, (unsigned)(k1 - k0) * sizeof(double2));
+                    }
+                }
+            }
+        }
         cs.seed(a, kc, a.normf[cls], true, M, Mp);
         fill_rc4(s_rc, M, M, Mp, lane);
 #pragma unroll
@@ -379,21 +401,23 @@ __global__ void __launch_bounds__(kWarps * 32, CS == 2 ? 4 : 1)
 }
 
 // Inverse DWT (see the header comment). Each lane ends with case 4n + t4 of its n-tiles at
-// columns cw*KW + 8p + g. The rows of 4-degree block b+1 are generated while block b is applied.
+// columns cw*KW + 8p + g. The rows of 8-degree block b+1 are generated while block b is
+// applied (two MMA k-steps of 4 degrees). Coefficients move through registers one 32-degree
+// chunk ahead of their use; the first chunk of the next class is fetched during this one.
 template <int KT, int TW, int CS>
 __global__ void __launch_bounds__(kWarps * 32, CS == 2 ? 3 : 1)
     dwt_inverse_kernel(const double2* __restrict__ coeffs, double2* __restrict__ X, const DwtArgs a)
 {
     using L = InvSmem<KT>;
     using TM = Team<KT, TW, CS>;
-    constexpr int KW = L::KW, DS = L::DS, NSUB8 = KW / 8, PPS = NSUB8 / 4;   // subtiles per step
+    constexpr int KW = L::KW, DS = L::DS, NSUB8 = KW / 8;
     constexpr int NT = TM::NT;
     constexpr int TT = 32 * TM::WARPS;           // team threads
     constexpr int PER = (8 * kLB + TT - 1) / TT; // coefficients fetched per thread per chunk
     extern __shared__ double smem[];
     const TM tm;
     const int lane = tm.lane, g = tm.g, t4 = tm.t4;
-    double* s_d = smem + L::d_off + (size_t)tm.warp * 2 * 4 * DS;
+    double* s_d = smem + L::d_off + (size_t)tm.warp * 2 * 8 * DS;
     double* s_rc = smem + L::rc_off + (size_t)tm.warp * kLB * 4;
     double* s_g = smem + L::g_off + (size_t)tm.team * 2 * kLB * 16;   // [2][kLB][16]
     const int B = a.B, N = a.N;
@@ -408,38 +432,44 @@ __global__ void __launch_bounds__(kWarps * 32, CS == 2 ? 3 : 1)
         cs.cb[j] = kc[j] < N ? a.cosb[kc[j]] : 0.0;
     }
 
+    // coefficients of class (M, Mp) for degrees l .. l+31, scaled and signed, into registers
+    double2 pf[PER];
+    auto fetch = [&](int M, int Mp, int l) {
+        const int nc = class_case_count(M, Mp);
+#pragma unroll
+        for (int i = 0; i < PER; ++i) {
+            const int e = tm.tl + i * TT, c = e / kLB, ld = l + (e - c * kLB);
+            double2 v = make_double2(0.0, 0.0);
+            if (e < 8 * kLB && c < nc && ld < B) {
+                const PairCase p = class_case(M, Mp, c, N);
+                const double f = norm * case_sign(p, ld, M);
+                const double2 x = __ldg(coeffs + coef_index(ld, p.m1, p.m2));
+                v = make_double2(f * x.x, f * x.y);
+            }
+            pf[i] = v;
+        }
+    };
+    auto stash = [&](int buf) {
+#pragma unroll
+        for (int i = 0; i < PER; ++i) {
+            const int e = tm.tl + i * TT, c = e / kLB, j = e - c * kLB;
+            if (e < 8 * kLB) *reinterpret_cast<double2*>(s_g + (buf * kLB + j) * 16 + 2 * c) = pf[i];
+        }
+    };
+
     const int T = gridDim.x * TM::PER_CTA;
     const int my = blockIdx.x * TM::PER_CTA + tm.team;
-    for (int r = 0;; ++r) {
-        const int cls = snake_class(r, T, my);
-        if (cls >= ncls) break;
-        int M, Mp;
+    int cls = snake_class(0, T, my);
+    int M = 0, Mp = 0;
+    if (cls < ncls) {
         class_orders(cls, M, Mp);
+        fetch(M, Mp, M);
+    }
+    for (int r = 0; cls < ncls; ++r) {
         const int nc = class_case_count(M, Mp);
-
-        // coefficients of degrees l .. l+31, scaled and signed, fetched into registers
-        double2 pf[PER];
-        auto fetch = [&](int l) {
-#pragma unroll
-            for (int i = 0; i < PER; ++i) {
-                const int e = tm.tl + i * TT, c = e / kLB, ld = l + (e - c * kLB);
-                double2 v = make_double2(0.0, 0.0);
-                if (e < 8 * kLB && c < nc && ld < B) {
-                    const PairCase p = class_case(M, Mp, c, N);
-                    const double f = norm * case_sign(p, ld, M);
-                    const double2 x = __ldg(coeffs + coef_index(ld, p.m1, p.m2));
-                    v = make_double2(f * x.x, f * x.y);
-                }
-                pf[i] = v;
-            }
-        };
-        auto stash = [&](int buf) {
-#pragma unroll
-            for (int i = 0; i < PER; ++i) {
-                const int e = tm.tl + i * TT, c = e / kLB, j = e - c * kLB;
-                if (e < 8 * kLB) *reinterpret_cast<double2*>(s_g + (buf * kLB + j) * 16 + 2 * c) = pf[i];
-            }
-        };
+        const int nxt = snake_class(r + 1, T, my);
+        int M2 = 0, Mp2 = 0;
+        if (nxt < ncls) class_orders(nxt, M2, Mp2);
 
         double acc[NSUB8][NT][2];
 #pragma unroll
@@ -447,37 +477,45 @@ __global__ void __launch_bounds__(kWarps * 32, CS == 2 ? 3 : 1)
 #pragma unroll
             for (int n = 0; n < NT; ++n) acc[p][n][0] = acc[p][n][1] = 0.0;
 
-        fetch(M);
         cs.seed(a, kc, a.normf[cls], false, M, Mp);
         team_sync<TM::WARPS>(tm.team);   // the previous class is done with s_g
-        stash(0);
+        stash(0);                        // chunk 0 (fetched ahead)
         fill_rc4(s_rc, M, M, Mp, lane);
 #pragma unroll
-        for (int s = 0; s < 4; ++s) gen_step<KT>(cs, s_d + s * DS, lane, s_rc + 4 * s);   // block 0
+        for (int s = 0; s < 8; ++s) gen_step<KT>(cs, s_d + s * DS, lane, s_rc + 4 * s);   // block 0
         team_sync<TM::WARPS>(tm.team);   // chunk 0 and block 0 rows visible
-        if (M + kLB < B) fetch(M + kLB);
-        const int nblk = (B - M + 3) >> 2;
+        if (M + kLB < B) fetch(M, Mp, M + kLB);
+        else if (nxt < ncls) fetch(M2, Mp2, M2);
+
+        const int nblk = (B - M + 7) >> 3;
         int cur = 0;
         for (int blk = 0; blk < nblk; ++blk) {
-            const int off = 4 * blk;
-            const double* dc = s_d + cur * 4 * DS;
-            double* dn = s_d + (cur ^ 1) * 4 * DS;
-            // B fragments: G[l0 + t4][v] of this warp's n-tiles (zero beyond the last degree)
+            const int off = 8 * blk;
+            const double* dc = s_d + cur * 8 * DS;
+            double* dn = s_d + (cur ^ 1) * 8 * DS;
+            // B fragments for the two k-steps (degrees off + t4 and off + 4 + t4)
             const double* gb = s_g + ((((off >> 5) & 1) * kLB) + (off & (kLB - 1)) + t4) * 16;
-            double bv[NT];
+            double bv0[NT], bv1[NT];
 #pragma unroll
-            for (int n = 0; n < NT; ++n) bv[n] = gb[8 * (CS == 2 ? tm.h : n) + g];
+            for (int n = 0; n < NT; ++n) {
+                const int v = 8 * (CS == 2 ? tm.h : n) + g;
+                bv0[n] = gb[v];
+                bv1[n] = gb[4 * 16 + v];
+            }
             auto mma_step = [&](int s) {
 #pragma unroll
-                for (int i = 0; i < PPS; ++i) {
-                    const int p = s * PPS + i;
-                    const double av = dc[t4 * DS + 8 * p + g];
+                for (int p = s; p < NSUB8; p += 8) {   // subtiles spread over the 8 steps
+                    const double av0 = dc[t4 * DS + 8 * p + g];
+                    const double av1 = dc[(4 + t4) * DS + 8 * p + g];
 #pragma unroll
-                    for (int n = 0; n < NT; ++n) dmma(acc[p][n][0], acc[p][n][1], av, bv[n]);
+                    for (int n = 0; n < NT; ++n) {
+                        dmma(acc[p][n][0], acc[p][n][1], av0, bv0[n]);
+                        dmma(acc[p][n][0], acc[p][n][1], av1, bv1[n]);
+                    }
                 }
             };
             if (blk + 1 < nblk) {
-                const int offn = off + 4;
+                const int offn = off + 8;
                 const bool boundary = (offn & (kLB - 1)) == 0;
                 if (boundary) {
                     // publish the prefetched chunk (its buffer was last read two chunks ago)
@@ -486,19 +524,20 @@ __global__ void __launch_bounds__(kWarps * 32, CS == 2 ? 3 : 1)
                 }
                 const double* rcb = s_rc + 4 * (offn & (kLB - 1));
 #pragma unroll
-                for (int s = 0; s < 4; ++s) {
+                for (int s = 0; s < 8; ++s) {
                     mma_step(s);
                     gen_step<KT>(cs, dn + s * DS, lane, rcb + 4 * s);
                 }
                 if (boundary) {
                     team_sync<TM::WARPS>(tm.team);   // new chunk visible; the old one no longer read
-                    if (M + offn + kLB < B) fetch(M + offn + kLB);
+                    if (M + offn + kLB < B) fetch(M, Mp, M + offn + kLB);
+                    else if (nxt < ncls) fetch(M2, Mp2, M2);
                 } else {
                     __syncwarp();
                 }
             } else {
 #pragma unroll
-                for (int s = 0; s < 4; ++s) mma_step(s);
+                for (int s = 0; s < 8; ++s) mma_step(s);
             }
             cur ^= 1;
         }
@@ -515,6 +554,9 @@ __global__ void __launch_bounds__(kWarps * 32, CS == 2 ? 3 : 1)
                 }
             }
         }
+        cls = nxt;
+        M = M2;
+        Mp = Mp2;
     }
 }
 
