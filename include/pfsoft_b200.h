@@ -77,6 +77,25 @@ int pfsoft_cuda_idsoft(const double* d_coeffs, int B, double* d_grid, void* d_wo
  * has to start at zero. Same layouts and results as pfsoft_cuda_dsoft. */
 int pfsoft_cuda_dsoft_noalloc(const double* d_grid, int B, double* d_coeffs, void* stream);
 
+/* ---- Batches of transforms, uneven bandwidths ------------------------------------------------
+ * No counterpart in the reference (which transforms one grid per call). A plan groups `count`
+ * transforms by bandwidth; each execution runs batched FFT passes per bandwidth and ONE
+ * persistent DWT launch over every (bandwidth, order class, transform block) item, longest
+ * first, in which one on-chip Wigner recurrence serves up to `transforms_per_cta` transforms
+ * (0 = default: 4 for B <= 64, 2 above). Bandwidths up to 128 share the fused launch; larger
+ * ones use the per-transform DWT. The sequence is captured once into a CUDA graph and replayed
+ * (flags bit 0 disables the graph). The plan owns one spectrum workspace per transform
+ * (pfsoft_batch_workspace_bytes). Pointer tables are host arrays of `count` device pointers in
+ * the caller's order; every buffer has the single-transform layouts above. Stream ordered.
+ * Calls on one plan are serialised by the plan. */
+typedef struct pfsoft_batch pfsoft_batch;
+int pfsoft_batch_create(const int* bandwidths, int count, int transforms_per_cta, int flags, pfsoft_batch** out);
+int pfsoft_batch_destroy(pfsoft_batch* batch);
+size_t pfsoft_batch_workspace_bytes(const pfsoft_batch* batch);
+int pfsoft_batch_transforms_per_cta(const pfsoft_batch* batch);
+int pfsoft_batch_dsoft(pfsoft_batch* batch, const double* const* d_grids, double* const* d_coeffs, void* stream);
+int pfsoft_batch_idsoft(pfsoft_batch* batch, const double* const* d_coeffs, double* const* d_grids, void* stream);
+
 /* ---- Host-resident drop-in (synchronous) ---------------------------------------------------
  * The same transforms on host buffers: copy in, transform, copy out, wait. Pinned host
  * buffers (cudaHostAlloc) make the copies asynchronous DMA; pageable ones work too.
@@ -107,6 +126,13 @@ int pfsoft_layer_wise_idft2_host(int cols, int rows, int lays, double* h_arr, do
  *   caller side if needed). weighted != 0 multiplies column k by w_B(k). */
 int pfsoft_cuda_quadrature_weights(int B, double* d_w, void* stream);
 int pfsoft_cuda_wigner_d_matrix(int B, int M, int Mp, int weighted, double* d_out, void* stream);
+
+/* ---- Seeded coefficients on the device -------------------------------------------------------
+ * Counterpart of rand(DSOFTFourierCoefficients&, ...) (include/PFSOFTlib_headers/random.hpp:80),
+ * which seeds from the clock; this one is reproducible: value i is a function of (seed, i).
+ * kind 0: re, im uniform in [-1, 1); kind 1: |f| = (1+l)^-power |N(0,1)|, uniform phase;
+ * kind 2: |f| = (1+l)^-power, uniform phase. Fills all B(4B^2-1)/3 packed values. */
+int pfsoft_cuda_random_coeffs(double* d_coeffs, int B, unsigned long long seed, int kind, double power, void* stream);
 
 /* ---- Diagnostics (no counterpart in the reference) -----------------------------------------
  * pfsoft_launch_count: number of CUDA kernels this library has launched in the process.

@@ -27,6 +27,12 @@ SIGNATURES = {
     "pfsoft_cuda_dsoft": (_c_int, [_vp, _c_int, _vp, _vp, _c_size, _vp]),
     "pfsoft_cuda_idsoft": (_c_int, [_vp, _c_int, _vp, _vp, _c_size, _vp]),
     "pfsoft_cuda_dsoft_noalloc": (_c_int, [_vp, _c_int, _vp, _vp]),
+    "pfsoft_batch_create": (_c_int, [_vp, _c_int, _c_int, _c_int, _vp]),
+    "pfsoft_batch_destroy": (_c_int, [_vp]),
+    "pfsoft_batch_workspace_bytes": (_c_size, [_vp]),
+    "pfsoft_batch_transforms_per_cta": (_c_int, [_vp]),
+    "pfsoft_batch_dsoft": (_c_int, [_vp, _vp, _vp, _vp]),
+    "pfsoft_batch_idsoft": (_c_int, [_vp, _vp, _vp, _vp]),
     "pfsoft_dsoft_host": (_c_int, [_vp, _c_int, _vp]),
     "pfsoft_idsoft_host": (_c_int, [_vp, _c_int, _vp]),
     "pfsoft_cuda_layer_wise_dft2": (_c_int, [_c_int, _c_int, _c_int, _vp, _c_double, _vp]),
@@ -35,6 +41,7 @@ SIGNATURES = {
     "pfsoft_layer_wise_idft2_host": (_c_int, [_c_int, _c_int, _c_int, _vp, _c_double]),
     "pfsoft_cuda_quadrature_weights": (_c_int, [_c_int, _vp, _vp]),
     "pfsoft_cuda_wigner_d_matrix": (_c_int, [_c_int, _c_int, _c_int, _c_int, _vp, _vp]),
+    "pfsoft_cuda_random_coeffs": (_c_int, [_vp, _c_int, ctypes.c_ulonglong, _c_int, _c_double, _vp]),
     "pfsoft_launch_count": (ctypes.c_longlong, []),
     "pfsoft_tune_dwt_case_split": (_c_int, [_c_int, _c_int]),
     "pfsoft_profile_enable": (_c_int, [_c_int]),

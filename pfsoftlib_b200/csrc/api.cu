@@ -171,6 +171,7 @@ int get_tables(int B, cudaStream_t stream, BandTables* out)
 
 namespace pfsoft_dev {
 void set_last_error(const char* msg) { g_last_error = msg; }
+int tables_for(int B, cudaStream_t s, BandTables* out);
 }  // namespace pfsoft_dev
 
 namespace {
@@ -200,7 +201,7 @@ int get_workspace(size_t bytes, void** ws)
 FftPassArgs pass_args(int n, int nvec, const BandTables& t, FftStrides src, FftStrides dst, double scale)
 {
     FftPassArgs a;
-    memset(&a, 0, sizeof(a));
+    memset(&a, 0, sizeof(a));   // srcs/dsts null: single transform
     a.n = n;
     a.nvec = nvec;
     a.kb = kFftKB;
@@ -390,6 +391,11 @@ __global__ void wigner_matrix_kernel(int B, int M, int Mp, const double* w, cons
 }
 
 }  // namespace
+
+namespace pfsoft_dev {
+// Cached tables of a bandwidth on the current device (used by the batch plans).
+int tables_for(int B, cudaStream_t s, BandTables* out) { return get_tables(B, s, out); }
+}  // namespace pfsoft_dev
 
 extern "C" {
 

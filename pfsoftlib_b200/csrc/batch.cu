@@ -1,0 +1,413 @@
+// Batched SO(3) transforms over many bandwidths (C ABI: pfsoft_batch_*).
+//
+// A batch plan groups its transforms by bandwidth. One forward execution is
+//   per group:  F1 (gamma DFT -> beta-innermost spectrum), F2 (alpha DFT)   [one launch each,
+//               gridDim.z = transforms of the group]
+//   all groups: one persistent DWT launch over every (group, order class, transform block)
+//               item, longest first (dwt_batch.cu)
+// and the inverse runs the mirror image. Groups above B = 128 run the per-transform DWT kernels.
+// The whole sequence is captured once into a CUDA graph; the device tables of grid and
+// coefficient pointers that the kernels read are refreshed before each replay, so one graph
+// serves any buffers.
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstring>
+#include <map>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/pfsoft_b200.h"
+#include "common.cuh"
+#include "dwt.cuh"
+#include "fft.cuh"
+
+using namespace pfsoft_dev;
+
+namespace pfsoft_dev {
+int tables_for(int B, cudaStream_t s, BandTables* out);   // api.cu: cached tables of a bandwidth
+}
+
+namespace {
+
+constexpr int kBatchMaxFused = 128;   // largest bandwidth of the fused DWT launch (N <= 256)
+
+__global__ void zero_nyquist_batched(double2* const* X, int B)
+{
+    double2* x = X[blockIdx.z];
+    const int N = 2 * B;
+    const long long total = (long long)(2 * N - 1) * N;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total; i += (long long)gridDim.x * blockDim.x) {
+        const long long v = i / N;
+        const int k = (int)(i - v * N);
+        int row, col;
+        if (v < N) {
+            row = B;
+            col = (int)v;
+        } else {
+            col = B;
+            row = (int)(v - N);
+            if (row >= B) ++row;
+        }
+        x[((size_t)row * N + col) * N + k] = make_double2(0.0, 0.0);
+    }
+}
+
+int fail(int status, const std::string& msg)
+{
+    set_last_error(msg.c_str());
+    return status;
+}
+
+}  // namespace
+
+struct pfsoft_batch {
+    struct Group {
+        int B = 0, N = 0;
+        std::vector<int> members;   // transform indices in the caller's order
+        BandTables tables;
+        size_t ptr_base = 0;        // offset of this group's entries in the pointer tables
+    };
+    int count = 0;
+    int tpc = 1;
+    int nmax = 0;
+    bool use_graph = true;
+    std::vector<Group> groups;
+    // device: pointer tables [3][count] (grid, coeffs, workspace) in group order
+    double2** d_ptr = nullptr;
+    double2** h_ptr = nullptr;   // pinned staging of the same
+    DwtGroup* d_groups_fwd = nullptr;
+    DwtGroup* d_groups_inv = nullptr;
+    DwtItem* d_items = nullptr;
+    int n_items = 0;
+    int* d_counter = nullptr;
+    void* ws = nullptr;
+    size_t ws_bytes = 0;
+    cudaGraphExec_t graph[2] = {nullptr, nullptr};
+    cudaEvent_t uploaded = nullptr;   // the last pointer upload has read h_ptr
+    std::mutex mu;
+
+    double2** grid_ptrs() const { return d_ptr; }
+    double2** coef_ptrs() const { return d_ptr + count; }
+    double2** ws_ptrs() const { return d_ptr + 2 * (size_t)count; }
+};
+
+namespace {
+
+// Sequence of one direction on stream s (captured into a graph, or run directly).
+int enqueue(pfsoft_batch* b, int dir, cudaStream_t s)
+{
+    const int sign = dir == 0 ? -1 : +1;
+    auto fft_group = [&](const pfsoft_batch::Group& g, bool first_pass) -> cudaError_t {
+        const int N = g.N;
+        const long long n = N, n2 = n * n;
+        FftPassArgs a;
+        memset(&a, 0, sizeof(a));
+        a.n = N;
+        a.nvec = N;
+        a.kb = 8;
+        a.nstages = fft_plan_radices(N, a.radix, a.ns);
+        a.twiddle = g.tables.twiddle;
+        a.scale = 1.0;
+        double2** grids = b->grid_ptrs() + g.ptr_base;
+        double2** wss = b->ws_ptrs() + g.ptr_base;
+        if (dir == 0) {
+            if (first_pass) {   // F1: grid -> spectrum (gamma DFT, beta innermost)
+                a.src = FftStrides{n2, n, 1};
+                a.dst = FftStrides{1, n, n2};
+                a.srcs = grids;
+                a.dsts = wss;
+            } else {            // F2: alpha DFT in place
+                a.src = a.dst = FftStrides{1, n2, n};
+                a.srcs = wss;
+                a.dsts = wss;
+            }
+        } else {
+            if (first_pass) {   // I2: inverse alpha DFT in place
+                a.src = a.dst = FftStrides{1, n2, n};
+                a.srcs = wss;
+                a.dsts = wss;
+            } else {            // I1: spectrum -> grid, scaled 1/(4B^2)
+                a.src = FftStrides{1, n, n2};
+                a.dst = FftStrides{n2, n, 1};
+                a.srcs = wss;
+                a.dsts = grids;
+                a.scale = 1.0 / (4.0 * g.B * g.B);
+            }
+        }
+        return fft_pass_launch(nullptr, nullptr, a, N, sign, s, (int)g.members.size());
+    };
+    auto dwt_large = [&](const pfsoft_batch::Group& g) -> cudaError_t {
+        // bandwidths above the fused launch: per-transform DWT kernels
+        DwtArgs a;
+        a.B = g.B;
+        a.N = g.N;
+        a.cosb = g.tables.cosb;
+        a.sinh = g.tables.sinh;
+        a.cosh = g.tables.cosh;
+        a.w = g.tables.w;
+        a.normf = g.tables.normf;
+        a.pw_sin = g.tables.pw_sin;
+        a.pw_cos = g.tables.pw_cos;
+        a.team_warps = dwt_team_warps(g.N);
+        for (size_t i = 0; i < g.members.size(); ++i) {
+            const int t = g.members[i];
+            double2* X = static_cast<double2*>(b->h_ptr[2 * (size_t)b->count + g.ptr_base + i]);
+            (void)t;
+            cudaError_t e = dir == 0 ? dwt_forward_launch(X, b->h_ptr[b->count + g.ptr_base + i], a, 0, s)
+                                     : dwt_inverse_launch(b->h_ptr[b->count + g.ptr_base + i], X, a, 0, s);
+            if (e != cudaSuccess) return e;
+        }
+        return cudaSuccess;
+    };
+    cudaError_t e = cudaSuccess;
+    if (dir == 0) {
+        for (const auto& g : b->groups)
+            if (e == cudaSuccess) e = fft_group(g, true);
+        for (const auto& g : b->groups)
+            if (e == cudaSuccess) e = fft_group(g, false);
+        if (e == cudaSuccess && b->n_items > 0) {
+            e = cudaMemsetAsync(b->d_counter, 0, sizeof(int), s);
+            if (e == cudaSuccess) e = dwt_batch_launch(0, b->d_groups_fwd, b->d_items, b->n_items, b->d_counter, b->tpc, b->nmax, s);
+        }
+        for (const auto& g : b->groups)
+            if (e == cudaSuccess && g.B > kBatchMaxFused) e = dwt_large(g);
+    } else {
+        for (const auto& g : b->groups) {
+            if (e != cudaSuccess) break;
+            const int N = g.N;
+            const long long total = (long long)(2 * N - 1) * N;
+            dim3 grid((unsigned)std::min<long long>((total + 255) / 256, 1024), 1, (unsigned)g.members.size());
+            zero_nyquist_batched<<<grid, 256, 0, s>>>(b->ws_ptrs() + g.ptr_base, g.B);
+            e = cudaGetLastError();
+        }
+        if (e == cudaSuccess && b->n_items > 0) {
+            e = cudaMemsetAsync(b->d_counter, 0, sizeof(int), s);
+            if (e == cudaSuccess) e = dwt_batch_launch(1, b->d_groups_inv, b->d_items, b->n_items, b->d_counter, b->tpc, b->nmax, s);
+        }
+        for (const auto& g : b->groups)
+            if (e == cudaSuccess && g.B > kBatchMaxFused) e = dwt_large(g);
+        for (const auto& g : b->groups)
+            if (e == cudaSuccess) e = fft_group(g, true);
+        for (const auto& g : b->groups)
+            if (e == cudaSuccess) e = fft_group(g, false);
+    }
+    if (e != cudaSuccess) return fail(PFSOFT_ECUDA, std::string("batch launch: ") + cudaGetErrorString(e));
+    return PFSOFT_OK;
+}
+
+void free_batch(pfsoft_batch* b)
+{
+    for (auto& g : b->graph)
+        if (g) cudaGraphExecDestroy(g);
+    if (b->uploaded) cudaEventDestroy(b->uploaded);
+    cudaFree(b->d_ptr);
+    cudaFreeHost(b->h_ptr);
+    cudaFree(b->d_groups_fwd);
+    cudaFree(b->d_groups_inv);
+    cudaFree(b->d_items);
+    cudaFree(b->d_counter);
+    cudaFree(b->ws);
+    delete b;
+}
+
+}  // namespace
+
+extern "C" {
+
+int pfsoft_batch_create(const int* bandwidths, int count, int transforms_per_cta, int flags, pfsoft_batch** out)
+{
+    set_last_error("");
+    if (!out) return fail(PFSOFT_EINVAL, "null output handle");
+    *out = nullptr;
+    if (!bandwidths || count < 1) return fail(PFSOFT_EINVAL, "batch needs at least one bandwidth");
+    if (transforms_per_cta != 0 && transforms_per_cta != 1 && transforms_per_cta != 2 && transforms_per_cta != 4)
+        return fail(PFSOFT_EINVAL, "transforms_per_cta must be 0 (auto), 1, 2 or 4");
+    for (int i = 0; i < count; ++i)
+        if (bandwidths[i] < 1 || bandwidths[i] > 512) return fail(PFSOFT_EINVAL, "bandwidth must be in [1, 512]");
+    pfsoft_batch* b = new pfsoft_batch();
+    b->count = count;
+    b->use_graph = (flags & 1) == 0;
+    std::map<int, std::vector<int> > by_b;
+    for (int i = 0; i < count; ++i) by_b[bandwidths[i]].push_back(i);
+    size_t base = 0, ws_total = 0;
+    std::vector<size_t> ws_off(count);
+    for (auto& kv : by_b) {
+        pfsoft_batch::Group g;
+        g.B = kv.first;
+        g.N = 2 * kv.first;
+        g.members = kv.second;
+        g.ptr_base = base;
+        base += g.members.size();
+        for (int t : g.members) {
+            ws_off[t] = ws_total;
+            ws_total += (size_t)g.N * g.N * g.N * sizeof(double2);
+        }
+        int rc = tables_for(g.B, nullptr, &g.tables);
+        if (rc) {
+            free_batch(b);
+            return rc;
+        }
+        if (g.B <= kBatchMaxFused) b->nmax = std::max(b->nmax, g.N);
+        b->groups.push_back(g);
+    }
+    b->tpc = transforms_per_cta ? transforms_per_cta : dwt_batch_transforms_per_cta(std::max(b->nmax, 2));
+    // work items, longest first: (B - M) degrees x N columns of beta x transforms
+    std::vector<DwtItem> items;
+    std::vector<double> cost;
+    std::vector<DwtGroup> dg_f, dg_i;
+    int gi_fused = 0;
+    std::vector<int> fused_index(b->groups.size(), -1);
+    for (size_t gi = 0; gi < b->groups.size(); ++gi) {
+        const auto& g = b->groups[gi];
+        if (g.B > kBatchMaxFused) continue;
+        fused_index[gi] = gi_fused++;
+        const int T = (int)g.members.size();
+        for (int c = 0; c < num_classes(g.B); ++c) {
+            int M, Mp;
+            class_orders(c, M, Mp);
+            for (int t0 = 0; t0 < T; t0 += b->tpc) {
+                DwtItem it;
+                it.group = fused_index[gi];
+                it.cls = c;
+                it.t0 = t0;
+                it.nt = std::min(b->tpc, T - t0);
+                items.push_back(it);
+                cost.push_back((double)(g.B - M) * g.N * it.nt + 64.0 * g.N);
+            }
+        }
+    }
+    std::vector<int> order(items.size());
+    for (size_t i = 0; i < order.size(); ++i) order[i] = (int)i;
+    std::stable_sort(order.begin(), order.end(), [&](int x, int y) { return cost[x] > cost[y]; });
+    std::vector<DwtItem> sorted(items.size());
+    for (size_t i = 0; i < order.size(); ++i) sorted[i] = items[order[i]];
+    b->n_items = (int)sorted.size();
+
+    cudaError_t e = cudaMalloc(&b->d_ptr, 3 * (size_t)count * sizeof(double2*));
+    if (e == cudaSuccess) e = cudaHostAlloc(&b->h_ptr, 3 * (size_t)count * sizeof(double2*), cudaHostAllocDefault);
+    if (e == cudaSuccess) e = cudaMalloc(&b->d_counter, sizeof(int));
+    if (e == cudaSuccess && !sorted.empty()) e = cudaMalloc(&b->d_items, sorted.size() * sizeof(DwtItem));
+    if (e == cudaSuccess) e = cudaMalloc(&b->ws, ws_total);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&b->uploaded, cudaEventDisableTiming);
+    if (e != cudaSuccess) {
+        free_batch(b);
+        return fail(PFSOFT_ENOMEM, std::string("batch allocation: ") + cudaGetErrorString(e));
+    }
+    b->ws_bytes = ws_total;
+    std::memset(b->h_ptr, 0, 3 * (size_t)count * sizeof(double2*));
+    for (const auto& g : b->groups)
+        for (size_t i = 0; i < g.members.size(); ++i)
+            b->h_ptr[2 * (size_t)count + g.ptr_base + i] =
+                reinterpret_cast<double2*>(static_cast<char*>(b->ws) + ws_off[g.members[i]]);
+    // group descriptors for the fused DWT (pointer tables inside the device array)
+    for (size_t gi = 0; gi < b->groups.size(); ++gi) {
+        const auto& g = b->groups[gi];
+        if (fused_index[gi] < 0) continue;
+        DwtGroup d;
+        d.B = g.B;
+        d.N = g.N;
+        d.T = (int)g.members.size();
+        d.cosb = g.tables.cosb;
+        d.w = g.tables.w;
+        d.normf = g.tables.normf;
+        d.pw_sin = g.tables.pw_sin;
+        d.pw_cos = g.tables.pw_cos;
+        d.X = b->ws_ptrs() + g.ptr_base;
+        d.coeffs = b->coef_ptrs() + g.ptr_base;
+        dg_f.push_back(d);
+        dg_i.push_back(d);
+    }
+    if (!dg_f.empty()) {
+        e = cudaMalloc(&b->d_groups_fwd, dg_f.size() * sizeof(DwtGroup));
+        if (e == cudaSuccess) e = cudaMalloc(&b->d_groups_inv, dg_i.size() * sizeof(DwtGroup));
+        if (e == cudaSuccess) e = cudaMemcpy(b->d_groups_fwd, dg_f.data(), dg_f.size() * sizeof(DwtGroup), cudaMemcpyHostToDevice);
+        if (e == cudaSuccess) e = cudaMemcpy(b->d_groups_inv, dg_i.data(), dg_i.size() * sizeof(DwtGroup), cudaMemcpyHostToDevice);
+        if (e == cudaSuccess) e = cudaMemcpy(b->d_items, sorted.data(), sorted.size() * sizeof(DwtItem), cudaMemcpyHostToDevice);
+    }
+    if (e == cudaSuccess) e = cudaMemcpy(b->d_ptr, b->h_ptr, 3 * (size_t)count * sizeof(double2*), cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) {
+        free_batch(b);
+        return fail(PFSOFT_ECUDA, std::string("batch setup: ") + cudaGetErrorString(e));
+    }
+    *out = b;
+    return PFSOFT_OK;
+}
+
+int pfsoft_batch_destroy(pfsoft_batch* b)
+{
+    if (!b) return PFSOFT_OK;
+    cudaDeviceSynchronize();
+    free_batch(b);
+    return PFSOFT_OK;
+}
+
+size_t pfsoft_batch_workspace_bytes(const pfsoft_batch* b) { return b ? b->ws_bytes : 0; }
+
+int pfsoft_batch_transforms_per_cta(const pfsoft_batch* b) { return b ? b->tpc : 0; }
+
+static int batch_run(pfsoft_batch* b, int dir, const double* const* in, double* const* out, void* stream)
+{
+    set_last_error("");
+    if (!b) return fail(PFSOFT_EINVAL, "null batch");
+    if (!in || !out) return fail(PFSOFT_EINVAL, "null pointer table");
+    std::lock_guard<std::mutex> lk(b->mu);
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    // the previous call's upload must have read the staging table before it is rewritten
+    cudaError_t e = cudaEventSynchronize(b->uploaded);
+    if (e != cudaSuccess) return fail(PFSOFT_ECUDA, std::string("pointer upload wait: ") + cudaGetErrorString(e));
+    // pointer tables in group order (forward: in = grids, out = coeffs; inverse: swapped)
+    for (const auto& g : b->groups)
+        for (size_t i = 0; i < g.members.size(); ++i) {
+            const int t = g.members[i];
+            if (!in[t] || !out[t]) return fail(PFSOFT_EINVAL, "null buffer in the pointer table");
+            double2* grid = reinterpret_cast<double2*>(const_cast<double*>(dir == 0 ? in[t] : out[t]));
+            double2* coef = reinterpret_cast<double2*>(const_cast<double*>(dir == 0 ? out[t] : in[t]));
+            b->h_ptr[g.ptr_base + i] = grid;
+            b->h_ptr[b->count + g.ptr_base + i] = coef;
+        }
+    e = cudaMemcpyAsync(b->d_ptr, b->h_ptr, 2 * (size_t)b->count * sizeof(double2*), cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess) e = cudaEventRecord(b->uploaded, s);
+    if (e != cudaSuccess) return fail(PFSOFT_ECUDA, std::string("pointer upload: ") + cudaGetErrorString(e));
+    bool large = false;
+    for (const auto& g : b->groups) large |= g.B > kBatchMaxFused;
+    // groups above the fused limit take their per-transform pointers at enqueue time, so they
+    // are launched directly; everything else replays one captured graph
+    if (!b->use_graph || large) {
+        // the host-side pointer table must stay valid until the launches are enqueued
+        return enqueue(b, dir, s);
+    }
+    if (!b->graph[dir]) {
+        cudaStream_t cs;
+        e = cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking);
+        if (e != cudaSuccess) return fail(PFSOFT_ECUDA, "capture stream");
+        cudaGraph_t graph = nullptr;
+        e = cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal);
+        int rc = PFSOFT_OK;
+        if (e == cudaSuccess) rc = enqueue(b, dir, cs);
+        cudaError_t e2 = cudaStreamEndCapture(cs, &graph);
+        if (e == cudaSuccess) e = e2;
+        if (e == cudaSuccess && rc == PFSOFT_OK) e = cudaGraphInstantiate(&b->graph[dir], graph, 0);
+        if (graph) cudaGraphDestroy(graph);
+        cudaStreamDestroy(cs);
+        if (rc != PFSOFT_OK) return rc;
+        if (e != cudaSuccess) return fail(PFSOFT_ECUDA, std::string("graph capture: ") + cudaGetErrorString(e));
+    }
+    e = cudaGraphLaunch(b->graph[dir], s);
+    if (e != cudaSuccess) return fail(PFSOFT_ECUDA, std::string("graph launch: ") + cudaGetErrorString(e));
+    return PFSOFT_OK;
+}
+
+int pfsoft_batch_dsoft(pfsoft_batch* b, const double* const* d_grids, double* const* d_coeffs, void* stream)
+{
+    return batch_run(b, 0, d_grids, d_coeffs, stream);
+}
+
+int pfsoft_batch_idsoft(pfsoft_batch* b, const double* const* d_coeffs, double* const* d_grids, void* stream)
+{
+    return batch_run(b, 1, d_coeffs, d_grids, stream);
+}
+
+}  // extern "C"

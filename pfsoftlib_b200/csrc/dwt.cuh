@@ -50,6 +50,33 @@ cudaError_t zero_nyquist_launch(double2* X, int B, cudaStream_t stream);
 // warp (warp pairs share the recurrence), 0 = default.
 void dwt_set_case_split(int dir, int cs);
 
+// ---- batched DWT over many transforms and bandwidths (dwt_batch.cu) -------------------------
+// A group holds T transforms of one bandwidth; X[t] is transform t's beta-innermost spectrum
+// (N^3) and coeffs[t] its packed coefficients. Forward reads X and writes coeffs, inverse the
+// other way. A work item is one order class of a group for transforms t0 .. t0+nt-1.
+struct DwtGroup {
+    int B, N, T;
+    const double* cosb;
+    const double* w;
+    const double* normf;
+    const double2* pw_sin;
+    const double2* pw_cos;
+    double2* const* X;
+    double2* const* coeffs;
+};
+
+struct DwtItem {
+    int group, cls, t0, nt;
+};
+
+// Transforms per CTA (1, 2 or 4) and the largest beta-column count the launch supports.
+int dwt_batch_transforms_per_cta(int nmax);
+size_t dwt_batch_smem_bytes(int direction, int tpc, int nmax);
+// One persistent launch over all items; *d_counter must be 0 (the kernel hands out items from
+// it). direction 0 = forward, 1 = inverse. nmax >= every group's N, nmax <= 256.
+cudaError_t dwt_batch_launch(int direction, const DwtGroup* d_groups, const DwtItem* d_items, int n_items,
+                             int* d_counter, int tpc, int nmax, cudaStream_t stream);
+
 // Sets the detail string returned by pfsoft_last_error() on the calling thread.
 void set_last_error(const char* msg);
 

@@ -247,6 +247,10 @@ __global__ void __launch_bounds__(256, 2) fft_pass_kernel(const double2* src, do
                                                        const FftPassArgs a)
 {
     extern __shared__ double2 smem[];
+    if (a.srcs) {
+        src = a.srcs[blockIdx.z];
+        dst = a.dsts[blockIdx.z];
+    }
     const int v0 = blockIdx.x * a.kb;
     const int nv = min(a.kb, a.nvec - v0);
     const long long src_base = (long long)v0 * a.src.sv + (long long)blockIdx.y * a.src.sb;
@@ -324,14 +328,14 @@ size_t fft_pass_smem_bytes(const FftPassArgs& a)
 }
 
 cudaError_t fft_pass_launch(const double2* src, double2* dst, const FftPassArgs& a, int ntiles, int sign,
-                            cudaStream_t stream)
+                            cudaStream_t stream, int nz)
 {
     // one butterfly per thread in the widest stage, up to 256 threads
     int widest = 1;
     for (int s = 0; s < a.nstages; ++s) widest = a.n / a.radix[s] > widest ? a.n / a.radix[s] : widest;
     int nthreads = ((a.kb * widest + 31) / 32) * 32;
     if (nthreads > 256) nthreads = 256;
-    dim3 grid((a.nvec + a.kb - 1) / a.kb, ntiles);
+    dim3 grid((a.nvec + a.kb - 1) / a.kb, ntiles, nz);
     size_t smem = fft_pass_smem_bytes(a);
     // the kernel indexes two buffers; with a single buffer the second pointer is never used
     if (sign < 0) {

@@ -25,14 +25,18 @@ struct FftPassArgs {
     FftStrides src, dst;
     double scale;                // applied to the stored values (1 = none)
     const double2* twiddle;      // twiddle[t] = exp(-2*pi*i*t/n), t < n
+    // batched passes: when set, transform z = blockIdx.z reads srcs[z] and writes dsts[z]
+    const double2* const* srcs;
+    double2* const* dsts;
 };
 
 // Radix plan for length n; returns the number of stages (0 if n cannot be planned).
 int fft_plan_radices(int n, int* radix, int* ns);
 
-// Launch one pass over a grid of (ceil(nvec/kb), ntiles) CTAs. sign = -1 forward, +1 inverse.
+// Launch one pass over a grid of (ceil(nvec/kb), ntiles, nz) CTAs. sign = -1 forward, +1 inverse.
+// nz > 1 requires a.srcs / a.dsts (one base pointer per transform).
 cudaError_t fft_pass_launch(const double2* src, double2* dst, const FftPassArgs& a, int ntiles, int sign,
-                            cudaStream_t stream);
+                            cudaStream_t stream, int nz = 1);
 
 size_t fft_pass_smem_bytes(const FftPassArgs& a);
 

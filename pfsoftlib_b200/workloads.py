@@ -1,0 +1,66 @@
+"""Runs one execution of a named workload through the C ABI (used for profiling and as a usage
+example). ``python -m pfsoftlib_b200.workloads <name> [reps]``:
+
+  single-<B>      IDSOFT then DSOFT of one transform at bandwidth B (PCG64-seeded inputs)
+  batch-<B>x<T>   a batch plan of T transforms at bandwidth B, IDSOFT then DSOFT
+  mixed           256 transforms, B uniform over {32,48,64,96,128} (seed 2), batched
+"""
+from __future__ import annotations
+
+import ctypes
+import sys
+
+import numpy as np
+
+
+def _coeffs(lib, B, seed, torch, s):
+    c = torch.empty(B * (4 * B * B - 1) // 3, dtype=torch.complex128, device="cuda")
+    assert lib.pfsoft_cuda_random_coeffs(c.data_ptr(), B, seed, 1, 1.0, s) == 0
+    return c
+
+
+def run(name: str, reps: int = 1) -> float:
+    import torch
+
+    from . import load
+
+    lib = load()
+    s = torch.cuda.current_stream().cuda_stream
+    if name.startswith("single-"):
+        B = int(name.split("-")[1])
+        N = 2 * B
+        c = _coeffs(lib, B, 1, torch, s)
+        g = torch.empty((N, N, N), dtype=torch.complex128, device="cuda")
+        f = torch.empty_like(c)
+        for _ in range(reps):
+            assert lib.pfsoft_cuda_idsoft(c.data_ptr(), B, g.data_ptr(), None, 0, s) == 0
+            assert lib.pfsoft_cuda_dsoft(g.data_ptr(), B, f.data_ptr(), None, 0, s) == 0
+        torch.cuda.synchronize()
+        return (f - c).abs().max().item()
+    if name.startswith("batch-") or name == "mixed":
+        if name == "mixed":
+            bws = [int(b) for b in np.random.default_rng(2).choice((32, 48, 64, 96, 128), size=256)]
+        else:
+            B, T = (int(x) for x in name.split("-")[1].split("x"))
+            bws = [B] * T
+        cs = [_coeffs(lib, B, 2000 + i, torch, s) for i, B in enumerate(bws)]
+        gs = [torch.empty((2 * B,) * 3, dtype=torch.complex128, device="cuda") for B in bws]
+        fs = [torch.empty_like(c) for c in cs]
+        plan = ctypes.c_void_p()
+        arr = (ctypes.c_int * len(bws))(*bws)
+        assert lib.pfsoft_batch_create(arr, len(bws), 0, 1, ctypes.byref(plan)) == 0
+        cp = (ctypes.c_void_p * len(bws))(*[t.data_ptr() for t in cs])
+        gp = (ctypes.c_void_p * len(bws))(*[t.data_ptr() for t in gs])
+        fp = (ctypes.c_void_p * len(bws))(*[t.data_ptr() for t in fs])
+        for _ in range(reps):
+            assert lib.pfsoft_batch_idsoft(plan, cp, gp, s) == 0
+            assert lib.pfsoft_batch_dsoft(plan, gp, fp, s) == 0
+        torch.cuda.synchronize()
+        lib.pfsoft_batch_destroy(plan)
+        return max((f - c).abs().max().item() for f, c in zip(fs, cs))
+    raise ValueError(f"unknown workload {name}")
+
+
+if __name__ == "__main__":
+    err = run(sys.argv[1], int(sys.argv[2]) if len(sys.argv) > 2 else 1)
+    print(f"{sys.argv[1]}: round-trip max abs {err:.3e}")
