@@ -35,7 +35,8 @@ typedef enum pfsoft_status {
     PFSOFT_ENOMEM = 2,   /* device or pinned allocation failed / budget exceeded */
     PFSOFT_ETIMEOUT = 3, /* a bounded wait ran out */
     PFSOFT_ECUDA = 4,    /* a CUDA runtime call failed */
-    PFSOFT_EBUSY = 5     /* a resource is in use (serving queue full) */
+    PFSOFT_EBUSY = 5,    /* a resource is in use (serving: request still queued or running) */
+    PFSOFT_ECANCELED = 6 /* serving: the request was cancelled before it reached the GPU */
 } pfsoft_status;
 
 const char* pfsoft_status_string(int status);
@@ -133,6 +134,57 @@ int pfsoft_cuda_wigner_d_matrix(int B, int M, int Mp, int weighted, double* d_ou
  * kind 0: re, im uniform in [-1, 1); kind 1: |f| = (1+l)^-power |N(0,1)|, uniform phase;
  * kind 2: |f| = (1+l)^-power, uniform phase. Fills all B(4B^2-1)/3 packed values. */
 int pfsoft_cuda_random_coeffs(double* d_coeffs, int B, unsigned long long seed, int kind, double power, void* stream);
+
+
+/* ---- Transform server (continuous batching) -----------------------------------------------
+ * No counterpart in the reference, which transforms one grid per call (src/fn_dsoft.cpp:76,
+ * src/fn_idsoft.cpp:72); each request here is one such call, queued.
+ * A server owns, on the device that is current at creation, one workspace arena of
+ * `budget_bytes` (admission is counted against it: a request runs when the spectrum it needs,
+ * pfsoft_workspace_bytes(B), fits), `streams` CUDA streams, and a scheduler thread. Requests
+ * name caller-owned device buffers that stay on the device; the caller keeps them alive and
+ * unchanged until the request finishes. The scheduler puts waiting requests of one direction
+ * and bandwidth into one batch (up to `max_batch`), launches it on a free stream as soon as a
+ * stream and arena space are free, and keeps doing so while earlier batches run, so work of
+ * requests that arrive later overlaps on the device with work already there.
+ *   direction 0: DSOFT, d_in = grid (2B)^3, d_out = coefficients.
+ *   direction 1: iDSOFT, d_in = coefficients, d_out = grid.
+ * submit: `stream` is where the caller produced d_in (NULL: the legacy default stream): the
+ *   request's batch waits for the work queued there before the call. The result is complete on
+ *   the device once poll / wait report PFSOFT_OK.
+ *   PFSOFT_ENOMEM if one transform of that bandwidth alone exceeds the budget (it is
+ *   rejected, not queued); PFSOFT_EBUSY after the server began shutting down.
+ * poll: PFSOFT_EBUSY while queued or running; otherwise the request's final status (PFSOFT_OK,
+ *   PFSOFT_ECANCELED, PFSOFT_ECUDA), returned once: the id is forgotten after that.
+ * wait: as poll, after waiting up to timeout_s seconds (PFSOFT_ETIMEOUT if still busy).
+ * cancel: PFSOFT_OK if the request was still queued (it then finishes as PFSOFT_ECANCELED),
+ *   PFSOFT_EBUSY if it is already on the GPU.
+ * pause(1) stops new launches (queued requests keep accumulating); pause(0) resumes.
+ * drain: waits until nothing is queued or running (PFSOFT_ETIMEOUT after timeout_s).
+ * destroy: cancels what is queued, waits for what runs, frees everything. */
+typedef struct pfsoft_server pfsoft_server;
+typedef struct pfsoft_server_stats {
+    long long submitted, completed, cancelled, rejected, failed;
+    long long batches;              /* batches launched */
+    double mean_batch;              /* transforms per batch */
+    double p50_ms, p99_ms, mean_ms, max_ms;   /* submit -> result on the device, per request */
+    double wall_s;                  /* first submit -> last completion since the last reset */
+    double transforms_per_s;        /* completed / wall_s */
+    size_t budget_bytes, peak_bytes;           /* arena capacity and high-water mark */
+    int max_concurrent_batches;     /* most batches on the device at one time */
+    int queued, running;            /* right now */
+} pfsoft_server_stats;
+int pfsoft_server_create(size_t budget_bytes, int max_batch, int streams, pfsoft_server** out);
+int pfsoft_server_destroy(pfsoft_server* srv);
+int pfsoft_server_submit(pfsoft_server* srv, int direction, int B, const double* d_in, double* d_out, void* stream,
+                         long long* id);
+int pfsoft_server_poll(pfsoft_server* srv, long long id);
+int pfsoft_server_wait(pfsoft_server* srv, long long id, double timeout_s);
+int pfsoft_server_cancel(pfsoft_server* srv, long long id);
+int pfsoft_server_pause(pfsoft_server* srv, int paused);
+int pfsoft_server_drain(pfsoft_server* srv, double timeout_s);
+int pfsoft_server_get_stats(pfsoft_server* srv, pfsoft_server_stats* out);
+int pfsoft_server_reset_stats(pfsoft_server* srv);
 
 /* ---- Diagnostics (no counterpart in the reference) -----------------------------------------
  * pfsoft_launch_count: number of CUDA kernels this library has launched in the process.

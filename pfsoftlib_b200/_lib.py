@@ -12,7 +12,7 @@ import threading
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libpfsoft_b200.so")
 
-PFSOFT_OK, PFSOFT_EINVAL, PFSOFT_ENOMEM, PFSOFT_ETIMEOUT, PFSOFT_ECUDA, PFSOFT_EBUSY = range(6)
+PFSOFT_OK, PFSOFT_EINVAL, PFSOFT_ENOMEM, PFSOFT_ETIMEOUT, PFSOFT_ECUDA, PFSOFT_EBUSY, PFSOFT_ECANCELED = range(7)
 
 _c_int, _c_size, _c_double, _vp = ctypes.c_int, ctypes.c_size_t, ctypes.c_double, ctypes.c_void_p
 
@@ -44,6 +44,16 @@ SIGNATURES = {
     "pfsoft_cuda_random_coeffs": (_c_int, [_vp, _c_int, ctypes.c_ulonglong, _c_int, _c_double, _vp]),
     "pfsoft_launch_count": (ctypes.c_longlong, []),
     "pfsoft_tune_dwt_case_split": (_c_int, [_c_int, _c_int]),
+    "pfsoft_server_create": (_c_int, [_c_size, _c_int, _c_int, _vp]),
+    "pfsoft_server_destroy": (_c_int, [_vp]),
+    "pfsoft_server_submit": (_c_int, [_vp, _c_int, _c_int, _vp, _vp, _vp, _vp]),
+    "pfsoft_server_poll": (_c_int, [_vp, ctypes.c_longlong]),
+    "pfsoft_server_wait": (_c_int, [_vp, ctypes.c_longlong, _c_double]),
+    "pfsoft_server_cancel": (_c_int, [_vp, ctypes.c_longlong]),
+    "pfsoft_server_pause": (_c_int, [_vp, _c_int]),
+    "pfsoft_server_drain": (_c_int, [_vp, _c_double]),
+    "pfsoft_server_get_stats": (_c_int, [_vp, _vp]),
+    "pfsoft_server_reset_stats": (_c_int, [_vp]),
     "pfsoft_profile_enable": (_c_int, [_c_int]),
     "pfsoft_profile_read": (_c_int, [_vp, _vp, _c_int]),
     "pfsoft_profile_stage_name": (ctypes.c_char_p, [_c_int]),

@@ -44,6 +44,7 @@ def up_to_date() -> bool:
         return False
     t = os.path.getmtime(LIB)
     deps = sources() + glob.glob(os.path.join(CSRC, "*.cuh")) + glob.glob(os.path.join(CSRC, "*.h")) + \
+        glob.glob(os.path.join(CSRC, "*.hpp")) + \
         glob.glob(os.path.join(ROOT, "include", "*.h"))
     return all(os.path.getmtime(d) <= t for d in deps)
 

@@ -408,6 +408,7 @@ const char* pfsoft_status_string(int status)
         case PFSOFT_ETIMEOUT: return "timed out";
         case PFSOFT_ECUDA: return "CUDA error";
         case PFSOFT_EBUSY: return "busy";
+        case PFSOFT_ECANCELED: return "cancelled";
         default: return "unknown status";
     }
 }

@@ -63,6 +63,132 @@ int fail(int status, const std::string& msg)
 
 }  // namespace
 
+
+namespace pfsoft_dev {
+
+// FFT pass of one same-bandwidth group: forward F1 (gamma DFT, grid -> beta-innermost spectrum)
+// and F2 (alpha DFT in place), inverse I2 (alpha, in place) and I1 (gamma, spectrum -> grid,
+// scaled 1/(4B^2)). grids / ws are device tables with one pointer per transform.
+FftPassArgs group_pass_args(int dir, bool first, const BandTables& t, double2** grids, double2** ws)
+{
+    const long long n = t.N, n2 = n * n;
+    FftPassArgs a;
+    memset(&a, 0, sizeof(a));
+    a.n = t.N;
+    a.nvec = t.N;
+    a.kb = 8;
+    a.nstages = fft_plan_radices(t.N, a.radix, a.ns);
+    a.twiddle = t.twiddle;
+    a.scale = 1.0;
+    if (dir == 0 && first) {          // F1
+        a.src = FftStrides{n2, n, 1};
+        a.dst = FftStrides{1, n, n2};
+        a.srcs = grids;
+        a.dsts = ws;
+    } else if (dir == 0 || first) {   // F2 / I2, in place
+        a.src = a.dst = FftStrides{1, n2, n};
+        a.srcs = ws;
+        a.dsts = ws;
+    } else {                          // I1
+        a.src = FftStrides{1, n, n2};
+        a.dst = FftStrides{n2, n, 1};
+        a.srcs = ws;
+        a.dsts = grids;
+        a.scale = 1.0 / (4.0 * t.B * t.B);
+    }
+    return a;
+}
+
+cudaError_t zero_nyquist_launch(double2** ws, int B, int T, cudaStream_t s)
+{
+    const int N = 2 * B;
+    const long long total = (long long)(2 * N - 1) * N;
+    dim3 grid((unsigned)std::min<long long>((total + 255) / 256, 1024), 1, (unsigned)T);
+    zero_nyquist_batched<<<grid, 256, 0, s>>>(ws, B);
+    return cudaGetLastError();
+}
+
+// Per-transform DWT launches of a group (bandwidths above the fused launch); X / coeffs are host
+// arrays of the device pointers.
+cudaError_t dwt_per_transform(int dir, const BandTables& t, int T, double2* const* X, double2* const* coeffs,
+                              cudaStream_t s)
+{
+    DwtArgs a;
+    a.B = t.B;
+    a.N = t.N;
+    a.cosb = t.cosb;
+    a.sinh = t.sinh;
+    a.cosh = t.cosh;
+    a.w = t.w;
+    a.normf = t.normf;
+    a.pw_sin = t.pw_sin;
+    a.pw_cos = t.pw_cos;
+    a.team_warps = dwt_team_warps(t.N);
+    for (int i = 0; i < T; ++i) {
+        cudaError_t e = dir == 0 ? dwt_forward_launch(X[i], coeffs[i], a, 0, s) : dwt_inverse_launch(coeffs[i], X[i], a, 0, s);
+        if (e != cudaSuccess) return e;
+    }
+    return cudaSuccess;
+}
+
+// One same-bandwidth group of T transforms in direction dir (0 forward, 1 inverse) on stream s.
+// d_grids / d_coefs / d_ws are device tables of T pointers; d_group describes the group for the
+// fused DWT and d_items lists its items (group_items); *d_counter is reset here. Bandwidths
+// above the fused launch use the per-transform kernels with the host copies h_coef / h_ws.
+int launch_group(int dir, const BandTables& t, int T, double2** d_grids, double2** d_ws, const DwtGroup* d_group,
+                 const DwtItem* d_items, int n_items, int* d_counter, int tpc, double2* const* h_coef,
+                 double2* const* h_ws, cudaStream_t s)
+{
+    const int sign = dir == 0 ? -1 : +1;
+    auto pass = [&](bool first) {
+        return fft_pass_launch(nullptr, nullptr, group_pass_args(dir, first, t, d_grids, d_ws), t.N, sign, s, T);
+    };
+    auto dwt = [&]() -> cudaError_t {
+        if (t.B > kBatchMaxFused) return dwt_per_transform(dir, t, T, h_ws, h_coef, s);
+        cudaError_t e = cudaMemsetAsync(d_counter, 0, sizeof(int), s);
+        if (e != cudaSuccess) return e;
+        return dwt_batch_launch(dir, d_group, d_items, n_items, d_counter, tpc, t.N <= 64 ? 64 : (t.N <= 128 ? 128 : 256), s);
+    };
+    cudaError_t e;
+    if (dir == 0) {
+        e = pass(true);
+        if (e == cudaSuccess) e = pass(false);
+        if (e == cudaSuccess) e = dwt();
+    } else {
+        e = zero_nyquist_launch(d_ws, t.B, T, s);
+        if (e == cudaSuccess) e = dwt();
+        if (e == cudaSuccess) e = pass(true);
+        if (e == cudaSuccess) e = pass(false);
+    }
+    if (e != cudaSuccess) return fail(PFSOFT_ECUDA, std::string("group launch: ") + cudaGetErrorString(e));
+    return PFSOFT_OK;
+}
+
+// Fused-DWT work items of one group of T transforms at bandwidth B, longest first.
+void group_items(int B, int T, int tpc, std::vector<DwtItem>& out)
+{
+    std::vector<std::pair<double, DwtItem> > v;
+    for (int c = 0; c < num_classes(B); ++c) {
+        int M, Mp;
+        class_orders(c, M, Mp);
+        for (int t0 = 0; t0 < T; t0 += tpc) {
+            DwtItem it;
+            it.group = 0;
+            it.cls = c;
+            it.t0 = t0;
+            it.nt = std::min(tpc, T - t0);
+            v.push_back(std::make_pair((double)(B - M) * it.nt + 64.0, it));
+        }
+    }
+    std::stable_sort(v.begin(), v.end(), [](const std::pair<double, DwtItem>& a, const std::pair<double, DwtItem>& b) {
+        return a.first > b.first;
+    });
+    out.clear();
+    for (auto& p : v) out.push_back(p.second);
+}
+
+}  // namespace pfsoft_dev
+
 struct pfsoft_batch {
     struct Group {
         int B = 0, N = 0;
@@ -101,66 +227,13 @@ int enqueue(pfsoft_batch* b, int dir, cudaStream_t s)
 {
     const int sign = dir == 0 ? -1 : +1;
     auto fft_group = [&](const pfsoft_batch::Group& g, bool first_pass) -> cudaError_t {
-        const int N = g.N;
-        const long long n = N, n2 = n * n;
-        FftPassArgs a;
-        memset(&a, 0, sizeof(a));
-        a.n = N;
-        a.nvec = N;
-        a.kb = 8;
-        a.nstages = fft_plan_radices(N, a.radix, a.ns);
-        a.twiddle = g.tables.twiddle;
-        a.scale = 1.0;
-        double2** grids = b->grid_ptrs() + g.ptr_base;
-        double2** wss = b->ws_ptrs() + g.ptr_base;
-        if (dir == 0) {
-            if (first_pass) {   // F1: grid -> spectrum (gamma DFT, beta innermost)
-                a.src = FftStrides{n2, n, 1};
-                a.dst = FftStrides{1, n, n2};
-                a.srcs = grids;
-                a.dsts = wss;
-            } else {            // F2: alpha DFT in place
-                a.src = a.dst = FftStrides{1, n2, n};
-                a.srcs = wss;
-                a.dsts = wss;
-            }
-        } else {
-            if (first_pass) {   // I2: inverse alpha DFT in place
-                a.src = a.dst = FftStrides{1, n2, n};
-                a.srcs = wss;
-                a.dsts = wss;
-            } else {            // I1: spectrum -> grid, scaled 1/(4B^2)
-                a.src = FftStrides{1, n, n2};
-                a.dst = FftStrides{n2, n, 1};
-                a.srcs = wss;
-                a.dsts = grids;
-                a.scale = 1.0 / (4.0 * g.B * g.B);
-            }
-        }
-        return fft_pass_launch(nullptr, nullptr, a, N, sign, s, (int)g.members.size());
+        FftPassArgs a = group_pass_args(dir, first_pass, g.tables, b->grid_ptrs() + g.ptr_base, b->ws_ptrs() + g.ptr_base);
+        return fft_pass_launch(nullptr, nullptr, a, g.N, sign, s, (int)g.members.size());
     };
     auto dwt_large = [&](const pfsoft_batch::Group& g) -> cudaError_t {
-        // bandwidths above the fused launch: per-transform DWT kernels
-        DwtArgs a;
-        a.B = g.B;
-        a.N = g.N;
-        a.cosb = g.tables.cosb;
-        a.sinh = g.tables.sinh;
-        a.cosh = g.tables.cosh;
-        a.w = g.tables.w;
-        a.normf = g.tables.normf;
-        a.pw_sin = g.tables.pw_sin;
-        a.pw_cos = g.tables.pw_cos;
-        a.team_warps = dwt_team_warps(g.N);
-        for (size_t i = 0; i < g.members.size(); ++i) {
-            const int t = g.members[i];
-            double2* X = static_cast<double2*>(b->h_ptr[2 * (size_t)b->count + g.ptr_base + i]);
-            (void)t;
-            cudaError_t e = dir == 0 ? dwt_forward_launch(X, b->h_ptr[b->count + g.ptr_base + i], a, 0, s)
-                                     : dwt_inverse_launch(b->h_ptr[b->count + g.ptr_base + i], X, a, 0, s);
-            if (e != cudaSuccess) return e;
-        }
-        return cudaSuccess;
+        const size_t c = (size_t)b->count;
+        return dwt_per_transform(dir, g.tables, (int)g.members.size(), b->h_ptr + 2 * c + g.ptr_base,
+                                 b->h_ptr + c + g.ptr_base, s);
     };
     cudaError_t e = cudaSuccess;
     if (dir == 0) {
@@ -175,14 +248,8 @@ int enqueue(pfsoft_batch* b, int dir, cudaStream_t s)
         for (const auto& g : b->groups)
             if (e == cudaSuccess && g.B > kBatchMaxFused) e = dwt_large(g);
     } else {
-        for (const auto& g : b->groups) {
-            if (e != cudaSuccess) break;
-            const int N = g.N;
-            const long long total = (long long)(2 * N - 1) * N;
-            dim3 grid((unsigned)std::min<long long>((total + 255) / 256, 1024), 1, (unsigned)g.members.size());
-            zero_nyquist_batched<<<grid, 256, 0, s>>>(b->ws_ptrs() + g.ptr_base, g.B);
-            e = cudaGetLastError();
-        }
+        for (const auto& g : b->groups)
+            if (e == cudaSuccess) e = zero_nyquist_launch(b->ws_ptrs() + g.ptr_base, g.B, (int)g.members.size(), s);
         if (e == cudaSuccess && b->n_items > 0) {
             e = cudaMemsetAsync(b->d_counter, 0, sizeof(int), s);
             if (e == cudaSuccess) e = dwt_batch_launch(1, b->d_groups_inv, b->d_items, b->n_items, b->d_counter, b->tpc, b->nmax, s);
