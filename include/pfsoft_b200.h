@@ -85,11 +85,21 @@ int pfsoft_cuda_dsoft_noalloc(const double* d_grid, int B, double* d_coeffs, voi
  * first, in which one on-chip Wigner recurrence serves up to `transforms_per_cta` transforms
  * (0 = default: 4 for B <= 64, 2 above). Bandwidths up to 128 share the fused launch; larger
  * ones use the per-transform DWT. The sequence is captured once into a CUDA graph and replayed
- * (flags bit 0 disables the graph). The plan owns one spectrum workspace per transform
- * (pfsoft_batch_workspace_bytes). Pointer tables are host arrays of `count` device pointers in
- * the caller's order; every buffer has the single-transform layouts above. Stream ordered.
- * Calls on one plan are serialised by the plan. */
+ * (PFSOFT_BATCH_NO_GRAPH disables the graph). The plan owns one spectrum workspace per
+ * transform (pfsoft_batch_workspace_bytes). Pointer tables are host arrays of `count` device
+ * pointers in the caller's order; every buffer has the single-transform layouts above. Stream
+ * ordered. Calls on one plan are serialised by the plan.
+ * PFSOFT_BATCH_SPLIT runs the DWT of the bandwidths that pfsoft_split_supported() accepts on the
+ * tensor cores instead: the FP64 Wigner rows and FP64 data are cut into six 8-bit digit planes
+ * held exactly in bf16, multiplied with FP32 accumulation (exact for the leading planes) and
+ * summed in FP64; relative L2 error about 1e-13 against the FP64 path. Four transforms of one
+ * bandwidth share each generated Wigner tile. pfsoft_batch_status reports PFSOFT_ETIMEOUT if a
+ * bounded wait inside that kernel ever ran out (it synchronises the device). */
+#define PFSOFT_BATCH_NO_GRAPH 1
+#define PFSOFT_BATCH_SPLIT 2
 typedef struct pfsoft_batch pfsoft_batch;
+int pfsoft_split_supported(int B);
+int pfsoft_batch_status(pfsoft_batch* batch);
 int pfsoft_batch_create(const int* bandwidths, int count, int transforms_per_cta, int flags, pfsoft_batch** out);
 int pfsoft_batch_destroy(pfsoft_batch* batch);
 size_t pfsoft_batch_workspace_bytes(const pfsoft_batch* batch);

@@ -33,6 +33,8 @@ SIGNATURES = {
     "pfsoft_batch_transforms_per_cta": (_c_int, [_vp]),
     "pfsoft_batch_dsoft": (_c_int, [_vp, _vp, _vp, _vp]),
     "pfsoft_batch_idsoft": (_c_int, [_vp, _vp, _vp, _vp]),
+    "pfsoft_split_supported": (_c_int, [_c_int]),
+    "pfsoft_batch_status": (_c_int, [_vp]),
     "pfsoft_dsoft_host": (_c_int, [_vp, _c_int, _vp]),
     "pfsoft_idsoft_host": (_c_int, [_vp, _c_int, _vp]),
     "pfsoft_cuda_layer_wise_dft2": (_c_int, [_c_int, _c_int, _c_int, _vp, _c_double, _vp]),

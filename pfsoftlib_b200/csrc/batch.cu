@@ -209,6 +209,12 @@ struct pfsoft_batch {
     DwtItem* d_items = nullptr;
     int n_items = 0;
     int* d_counter = nullptr;
+    // split-precision DWT (PFSOFT_BATCH_SPLIT): items of the groups it takes, its counter and
+    // the sticky status of its bounded waits
+    void* d_split_fwd = nullptr;
+    void* d_split_inv = nullptr;
+    int n_split_fwd = 0, n_split_inv = 0;
+    int* d_split = nullptr;   // [0] counter, [1] status
     void* ws = nullptr;
     size_t ws_bytes = 0;
     cudaGraphExec_t graph[2] = {nullptr, nullptr};
@@ -245,6 +251,10 @@ int enqueue(pfsoft_batch* b, int dir, cudaStream_t s)
             e = cudaMemsetAsync(b->d_counter, 0, sizeof(int), s);
             if (e == cudaSuccess) e = dwt_batch_launch(0, b->d_groups_fwd, b->d_items, b->n_items, b->d_counter, b->tpc, b->nmax, s);
         }
+        if (e == cudaSuccess && b->n_split_fwd > 0) {
+            e = cudaMemsetAsync(b->d_split, 0, sizeof(int), s);
+            if (e == cudaSuccess) e = dwt_split_launch(0, b->d_groups_fwd, b->d_split_fwd, b->n_split_fwd, b->d_split, b->d_split + 1, s);
+        }
         for (const auto& g : b->groups)
             if (e == cudaSuccess && g.B > kBatchMaxFused) e = dwt_large(g);
     } else {
@@ -253,6 +263,10 @@ int enqueue(pfsoft_batch* b, int dir, cudaStream_t s)
         if (e == cudaSuccess && b->n_items > 0) {
             e = cudaMemsetAsync(b->d_counter, 0, sizeof(int), s);
             if (e == cudaSuccess) e = dwt_batch_launch(1, b->d_groups_inv, b->d_items, b->n_items, b->d_counter, b->tpc, b->nmax, s);
+        }
+        if (e == cudaSuccess && b->n_split_inv > 0) {
+            e = cudaMemsetAsync(b->d_split, 0, sizeof(int), s);
+            if (e == cudaSuccess) e = dwt_split_launch(1, b->d_groups_inv, b->d_split_inv, b->n_split_inv, b->d_split, b->d_split + 1, s);
         }
         for (const auto& g : b->groups)
             if (e == cudaSuccess && g.B > kBatchMaxFused) e = dwt_large(g);
@@ -276,6 +290,9 @@ void free_batch(pfsoft_batch* b)
     cudaFree(b->d_groups_inv);
     cudaFree(b->d_items);
     cudaFree(b->d_counter);
+    cudaFree(b->d_split_fwd);
+    cudaFree(b->d_split_inv);
+    cudaFree(b->d_split);
     cudaFree(b->ws);
     delete b;
 }
@@ -321,17 +338,31 @@ int pfsoft_batch_create(const int* bandwidths, int count, int transforms_per_cta
         b->groups.push_back(g);
     }
     b->tpc = transforms_per_cta ? transforms_per_cta : dwt_batch_transforms_per_cta(std::max(b->nmax, 2));
+    const bool split = (flags & PFSOFT_BATCH_SPLIT) != 0;
     // work items, longest first: (B - M) degrees x N columns of beta x transforms
     std::vector<DwtItem> items;
     std::vector<double> cost;
     std::vector<DwtGroup> dg_f, dg_i;
     int gi_fused = 0;
     std::vector<int> fused_index(b->groups.size(), -1);
+    std::vector<unsigned char> split_f, split_i;   // forward items, then inverse items
+    int n_split_f = 0, n_split_i = 0;
     for (size_t gi = 0; gi < b->groups.size(); ++gi) {
         const auto& g = b->groups[gi];
         if (g.B > kBatchMaxFused) continue;
         fused_index[gi] = gi_fused++;
         const int T = (int)g.members.size();
+        if (split && dwt_split_supported(g.B)) {
+            std::vector<unsigned char> v;
+            int n = 0;
+            dwt_split_items(0, fused_index[gi], g.B, T, v, &n);
+            split_f.insert(split_f.end(), v.begin(), v.end());
+            n_split_f += n;
+            dwt_split_items(1, fused_index[gi], g.B, T, v, &n);
+            split_i.insert(split_i.end(), v.begin(), v.end());
+            n_split_i += n;
+            continue;
+        }
         for (int c = 0; c < num_classes(g.B); ++c) {
             int M, Mp;
             class_orders(c, M, Mp);
@@ -359,9 +390,22 @@ int pfsoft_batch_create(const int* bandwidths, int count, int transforms_per_cta
     if (e == cudaSuccess && !sorted.empty()) e = cudaMalloc(&b->d_items, sorted.size() * sizeof(DwtItem));
     if (e == cudaSuccess) e = cudaMalloc(&b->ws, ws_total);
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&b->uploaded, cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaMalloc(&b->d_split, 2 * sizeof(int));
+    if (e == cudaSuccess && n_split_f > 0) e = cudaMalloc(&b->d_split_fwd, split_f.size());
+    if (e == cudaSuccess && n_split_i > 0) e = cudaMalloc(&b->d_split_inv, split_i.size());
     if (e != cudaSuccess) {
         free_batch(b);
         return fail(PFSOFT_ENOMEM, std::string("batch allocation: ") + cudaGetErrorString(e));
+    }
+    b->n_split_fwd = n_split_f;
+    b->n_split_inv = n_split_i;
+    e = cudaMemset(b->d_split, 0, 2 * sizeof(int));
+    if (e == cudaSuccess && (n_split_f > 0 || n_split_i > 0)) e = dwt_split_prepare();
+    if (e == cudaSuccess && n_split_f > 0) e = cudaMemcpy(b->d_split_fwd, split_f.data(), split_f.size(), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess && n_split_i > 0) e = cudaMemcpy(b->d_split_inv, split_i.data(), split_i.size(), cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) {
+        free_batch(b);
+        return fail(PFSOFT_ECUDA, std::string("batch setup: ") + cudaGetErrorString(e));
     }
     b->ws_bytes = ws_total;
     std::memset(b->h_ptr, 0, 3 * (size_t)count * sizeof(double2*));
@@ -392,7 +436,8 @@ int pfsoft_batch_create(const int* bandwidths, int count, int transforms_per_cta
         if (e == cudaSuccess) e = cudaMalloc(&b->d_groups_inv, dg_i.size() * sizeof(DwtGroup));
         if (e == cudaSuccess) e = cudaMemcpy(b->d_groups_fwd, dg_f.data(), dg_f.size() * sizeof(DwtGroup), cudaMemcpyHostToDevice);
         if (e == cudaSuccess) e = cudaMemcpy(b->d_groups_inv, dg_i.data(), dg_i.size() * sizeof(DwtGroup), cudaMemcpyHostToDevice);
-        if (e == cudaSuccess) e = cudaMemcpy(b->d_items, sorted.data(), sorted.size() * sizeof(DwtItem), cudaMemcpyHostToDevice);
+        if (e == cudaSuccess && !sorted.empty())
+            e = cudaMemcpy(b->d_items, sorted.data(), sorted.size() * sizeof(DwtItem), cudaMemcpyHostToDevice);
     }
     if (e == cudaSuccess) e = cudaMemcpy(b->d_ptr, b->h_ptr, 3 * (size_t)count * sizeof(double2*), cudaMemcpyHostToDevice);
     if (e != cudaSuccess) {
@@ -414,6 +459,18 @@ int pfsoft_batch_destroy(pfsoft_batch* b)
 size_t pfsoft_batch_workspace_bytes(const pfsoft_batch* b) { return b ? b->ws_bytes : 0; }
 
 int pfsoft_batch_transforms_per_cta(const pfsoft_batch* b) { return b ? b->tpc : 0; }
+
+int pfsoft_split_supported(int B) { return dwt_split_supported(B) ? 1 : 0; }
+
+int pfsoft_batch_status(pfsoft_batch* b)
+{
+    if (!b) return fail(PFSOFT_EINVAL, "null batch");
+    int st[2] = {0, 0};
+    cudaError_t e = cudaDeviceSynchronize();
+    if (e == cudaSuccess) e = cudaMemcpy(st, b->d_split, sizeof(st), cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess) return fail(PFSOFT_ECUDA, std::string("batch status: ") + cudaGetErrorString(e));
+    return st[1] ? fail(PFSOFT_ETIMEOUT, "a bounded wait in the split-precision DWT ran out") : PFSOFT_OK;
+}
 
 static int batch_run(pfsoft_batch* b, int dir, const double* const* in, double* const* out, void* stream)
 {

@@ -3,6 +3,8 @@
 
 #include <cuda_runtime.h>
 
+#include <vector>
+
 namespace pfsoft_dev {
 
 // Per-bandwidth constant tables, built once on the device (tables_build) and cached.
@@ -76,6 +78,16 @@ size_t dwt_batch_smem_bytes(int direction, int tpc, int nmax);
 // it). direction 0 = forward, 1 = inverse. nmax >= every group's N, nmax <= 256.
 cudaError_t dwt_batch_launch(int direction, const DwtGroup* d_groups, const DwtItem* d_items, int n_items,
                              int* d_counter, int tpc, int nmax, cudaStream_t stream);
+
+// Split-precision DWT on the tensor cores (dwt_split.cu) for groups whose bandwidth passes
+// dwt_split_supported. Items (opaque, dwt_split_items) of group index `group` in d_groups; one
+// persistent launch; *d_counter must be 0; a wait that ran out sets *d_status to 1.
+bool dwt_split_supported(int B);
+void dwt_split_items(int direction, int group, int B, int T, std::vector<unsigned char>& out, int* n_items);
+size_t dwt_split_item_bytes();
+cudaError_t dwt_split_prepare();   // kernel attributes; call once before any capture
+cudaError_t dwt_split_launch(int direction, const DwtGroup* d_groups, const void* d_items, int n_items, int* d_counter,
+                             int* d_status, cudaStream_t stream);
 
 // Sets the detail string returned by pfsoft_last_error() on the calling thread.
 void set_last_error(const char* msg);
