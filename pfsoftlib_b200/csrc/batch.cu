@@ -195,6 +195,7 @@ struct pfsoft_batch {
         std::vector<int> members;   // transform indices in the caller's order
         BandTables tables;
         size_t ptr_base = 0;        // offset of this group's entries in the pointer tables
+        bool split = false;         // DWT on the split-precision tensor-core kernel
     };
     int count = 0;
     int tpc = 1;
@@ -251,6 +252,9 @@ int enqueue(pfsoft_batch* b, int dir, cudaStream_t s)
             e = cudaMemsetAsync(b->d_counter, 0, sizeof(int), s);
             if (e == cudaSuccess) e = dwt_batch_launch(0, b->d_groups_fwd, b->d_items, b->n_items, b->d_counter, b->tpc, b->nmax, s);
         }
+        for (const auto& g : b->groups)
+            if (e == cudaSuccess && g.split)
+                e = dwt_split_scales(0, g.B, (int)g.members.size(), b->ws_ptrs() + g.ptr_base, b->coef_ptrs() + g.ptr_base, s);
         if (e == cudaSuccess && b->n_split_fwd > 0) {
             e = cudaMemsetAsync(b->d_split, 0, sizeof(int), s);
             if (e == cudaSuccess) e = dwt_split_launch(0, b->d_groups_fwd, b->d_split_fwd, b->n_split_fwd, b->d_split, b->d_split + 1, s);
@@ -264,6 +268,9 @@ int enqueue(pfsoft_batch* b, int dir, cudaStream_t s)
             e = cudaMemsetAsync(b->d_counter, 0, sizeof(int), s);
             if (e == cudaSuccess) e = dwt_batch_launch(1, b->d_groups_inv, b->d_items, b->n_items, b->d_counter, b->tpc, b->nmax, s);
         }
+        for (const auto& g : b->groups)
+            if (e == cudaSuccess && g.split)
+                e = dwt_split_scales(1, g.B, (int)g.members.size(), b->ws_ptrs() + g.ptr_base, b->coef_ptrs() + g.ptr_base, s);
         if (e == cudaSuccess && b->n_split_inv > 0) {
             e = cudaMemsetAsync(b->d_split, 0, sizeof(int), s);
             if (e == cudaSuccess) e = dwt_split_launch(1, b->d_groups_inv, b->d_split_inv, b->n_split_inv, b->d_split, b->d_split + 1, s);
@@ -325,9 +332,10 @@ int pfsoft_batch_create(const int* bandwidths, int count, int transforms_per_cta
         g.members = kv.second;
         g.ptr_base = base;
         base += g.members.size();
+        g.split = (flags & PFSOFT_BATCH_SPLIT) && g.B <= kBatchMaxFused && dwt_split_supported(g.B);
         for (int t : g.members) {
             ws_off[t] = ws_total;
-            ws_total += (size_t)g.N * g.N * g.N * sizeof(double2);
+            ws_total += ((size_t)g.N * g.N * g.N + (g.split ? dwt_split_aux_elems(g.B) : 0)) * sizeof(double2);
         }
         int rc = tables_for(g.B, nullptr, &g.tables);
         if (rc) {
@@ -338,7 +346,6 @@ int pfsoft_batch_create(const int* bandwidths, int count, int transforms_per_cta
         b->groups.push_back(g);
     }
     b->tpc = transforms_per_cta ? transforms_per_cta : dwt_batch_transforms_per_cta(std::max(b->nmax, 2));
-    const bool split = (flags & PFSOFT_BATCH_SPLIT) != 0;
     // work items, longest first: (B - M) degrees x N columns of beta x transforms
     std::vector<DwtItem> items;
     std::vector<double> cost;
@@ -352,7 +359,7 @@ int pfsoft_batch_create(const int* bandwidths, int count, int transforms_per_cta
         if (g.B > kBatchMaxFused) continue;
         fused_index[gi] = gi_fused++;
         const int T = (int)g.members.size();
-        if (split && dwt_split_supported(g.B)) {
+        if (g.split) {
             std::vector<unsigned char> v;
             int n = 0;
             dwt_split_items(0, fused_index[gi], g.B, T, v, &n);

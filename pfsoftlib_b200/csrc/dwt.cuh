@@ -86,6 +86,12 @@ bool dwt_split_supported(int B);
 void dwt_split_items(int direction, int group, int B, int T, std::vector<unsigned char>& out, int* n_items);
 size_t dwt_split_item_bytes();
 cudaError_t dwt_split_prepare();   // kernel attributes; call once before any capture
+// The split kernels read operand scales from a table of dwt_split_aux_elems(B) double2 that
+// follows each transform's spectrum (N^3 double2) in its workspace; dwt_split_scales fills it
+// (forward: from the spectra, after the FFT passes; inverse: from the coefficients).
+size_t dwt_split_aux_elems(int B);
+cudaError_t dwt_split_scales(int direction, int B, int T, double2* const* d_ws, const double2* const* d_coeffs,
+                             cudaStream_t stream);
 cudaError_t dwt_split_launch(int direction, const DwtGroup* d_groups, const void* d_items, int n_items, int* d_counter,
                              int* d_status, cudaStream_t stream);
 

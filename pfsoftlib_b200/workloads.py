@@ -4,6 +4,7 @@ example). ``python -m pfsoftlib_b200.workloads <name> [reps]``:
   single-<B>      IDSOFT then DSOFT of one transform at bandwidth B (PCG64-seeded inputs)
   batch-<B>x<T>   a batch plan of T transforms at bandwidth B, IDSOFT then DSOFT
   mixed           256 transforms, B uniform over {32,48,64,96,128} (seed 2), batched
+  <name>-split    a batch or mixed workload through the split-precision tensor-core DWT
 """
 from __future__ import annotations
 
@@ -37,6 +38,9 @@ def run(name: str, reps: int = 1) -> float:
             assert lib.pfsoft_cuda_dsoft(g.data_ptr(), B, f.data_ptr(), None, 0, s) == 0
         torch.cuda.synchronize()
         return (f - c).abs().max().item()
+    split = name.endswith("-split")
+    if split:
+        name = name[: -len("-split")]
     if name.startswith("batch-") or name == "mixed":
         if name == "mixed":
             bws = [int(b) for b in np.random.default_rng(2).choice((32, 48, 64, 96, 128), size=256)]
@@ -48,7 +52,7 @@ def run(name: str, reps: int = 1) -> float:
         fs = [torch.empty_like(c) for c in cs]
         plan = ctypes.c_void_p()
         arr = (ctypes.c_int * len(bws))(*bws)
-        assert lib.pfsoft_batch_create(arr, len(bws), 0, 1, ctypes.byref(plan)) == 0
+        assert lib.pfsoft_batch_create(arr, len(bws), 0, 1 | (2 if split else 0), ctypes.byref(plan)) == 0
         cp = (ctypes.c_void_p * len(bws))(*[t.data_ptr() for t in cs])
         gp = (ctypes.c_void_p * len(bws))(*[t.data_ptr() for t in gs])
         fp = (ctypes.c_void_p * len(bws))(*[t.data_ptr() for t in fs])
