@@ -67,8 +67,12 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="pfsoft", choices=["pfsoft", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", default="single", choices=["single", "mixed"],
-                    help="single: the B=128 headline; mixed: 256 transforms of uneven bandwidth, batched vs plain loop")
+    ap.add_argument("--workload", default="single", choices=["single", "mixed", "serve"],
+                    help="single: the B=128 headline; mixed: 256 transforms of uneven bandwidth, batched "
+                         "(FP64 and split precision) and served vs plain loop; serve: Poisson sweep of the server")
+    ap.add_argument("--rates", default="50,100,200,500,1000,2000", help="serve: offered requests/s")
+    ap.add_argument("--seconds", type=float, default=2.0, help="serve: arrival window per rate")
+    ap.add_argument("--budget-gb", type=float, default=64.0, help="serve: HBM budget of the server's arena")
     return ap.parse_args()
 
 
@@ -329,6 +333,21 @@ def run_mixed(args):
         nrm = torch.linalg.vector_norm(plain_back[i]).item()
         worst_vs = max(worst_vs, torch.linalg.vector_norm(back[i] - plain_back[i]).item() / nrm)
     lib.pfsoft_batch_destroy(plan)
+    # the same batch with the split-precision tensor-core DWT
+    plan_s = ctypes.c_void_p()
+    assert lib.pfsoft_batch_create(arr, len(bws), tpc, 2, ctypes.byref(plan_s)) == 0, lib.pfsoft_last_error()
+
+    def split():
+        assert lib.pfsoft_batch_idsoft(plan_s, cp, gp, s) == 0
+        assert lib.pfsoft_batch_dsoft(plan_s, gp, bp, s) == 0
+
+    ms_split = timed(split, steps)
+    split_status = lib.pfsoft_batch_status(plan_s)
+    lib.pfsoft_batch_destroy(plan_s)
+    split_vs, split_rt = 0.0, 0.0
+    for i in range(len(bws)):
+        split_vs = max(split_vs, (torch.linalg.vector_norm(back[i] - plain_back[i]) / torch.linalg.vector_norm(plain_back[i])).item())
+        split_rt = max(split_rt, (torch.linalg.vector_norm(back[i] - coeffs[i]) / torch.linalg.vector_norm(coeffs[i])).item())
     served = run_served(lib, bws, coeffs, grids, plain_back, ms_plain)
     n = 2 * len(bws)
     line = {
@@ -341,10 +360,97 @@ def run_mixed(args):
                    "l2": "working set ~45 GB, far above L2"},
         "plain_loop": {"value": n / (ms_plain / 1e3), "ms_per_step": ms_plain},
         "speedup_vs_plain_loop": ms_plain / ms_batch,
+        "split_precision": {"value": n / (ms_split / 1e3), "ms_per_step": ms_split,
+                            "speedup_vs_plain_loop": ms_plain / ms_split, "rel_l2_vs_fp64_max": split_vs,
+                            "round_trip_rel_l2_max": split_rt, "status": split_status,
+                            "note": "DWT as bf16 digit-plane products on tcgen05, FP32 accumulation, FP64 sum"},
         "served": served,
         "autotune": {"transforms_per_cta": tpc, "round_trip_ms": timings},
         "accuracy": {"round_trip_max_abs": worst_rt, "batched_vs_plain_rel_l2_max": worst_vs},
         "clocks": clk,
+    }
+    print(json.dumps(line), flush=True)
+
+
+SERVE_BANDS = (16, 24, 32, 48, 64, 96, 128, 192, 256)   # log-spaced: equal weights = log-uniform
+
+
+def run_serve_sweep(args):
+    """Serving under Poisson arrivals: requests 50/50 DSOFT / iDSOFT, bandwidth log-uniform over
+    16..256 (on the log-spaced grid SERVE_BANDS, PCG64 seed 4), offered at each rate of --rates for
+    --seconds. Inputs per bandwidth are generated once on the device; each request writes one of
+    four output buffers of its (bandwidth, direction), and waits for that buffer's previous request
+    before reusing it. Per rate: achieved transforms/s and p50 / p99 latency (submit -> result,
+    host clock at the server's completion callback)."""
+    import numpy as np
+    import torch
+
+    import pfsoftlib_b200
+    from pfsoftlib_b200.serving import TransformServer
+
+    lib = pfsoftlib_b200.load()
+    torch.cuda.set_device(0)
+    s = torch.cuda.current_stream().cuda_stream
+    pool = 4
+    ins, outs = {}, {}
+    for B in SERVE_BANDS:
+        c = torch.empty(B * (4 * B * B - 1) // 3, dtype=torch.complex128, device="cuda")
+        assert lib.pfsoft_cuda_random_coeffs(c.data_ptr(), B, 4000 + B, 2, 1.5, s) == 0
+        g = torch.empty((2 * B,) * 3, dtype=torch.complex128, device="cuda")
+        assert lib.pfsoft_cuda_idsoft(c.data_ptr(), B, g.data_ptr(), None, 0, s) == 0
+        ins[B] = (g, c)                     # direction 0 reads the grid, 1 the coefficients
+        outs[B] = ([torch.empty_like(c) for _ in range(pool)], [torch.empty_like(g) for _ in range(pool)])
+    torch.cuda.synchronize()
+    rng = np.random.default_rng(4)
+    rates = [float(r) for r in args.rates.split(",") if r]
+    sweep = []
+    budget = int(args.budget_gb * (1 << 30))
+    with TransformServer(budget_bytes=budget, max_batch=16, streams=4) as srv:
+        # warm-up: tables and item lists of every bandwidth and direction
+        warm = [srv.submit(d, B, ins[B][d], outs[B][d][0]) for B in SERVE_BANDS for d in (0, 1)]
+        for r in warm:
+            r.wait(300)
+        for rate in rates:
+            n = max(20, int(rate * args.seconds))
+            Bs = rng.choice(SERVE_BANDS, size=n)
+            dirs = rng.integers(0, 2, size=n)
+            gaps = rng.exponential(1.0 / rate, size=n)
+            slot = {}
+            last = {}
+            srv.reset_stats()
+            t0 = time.perf_counter()
+            due = t0 + np.cumsum(gaps)
+            reqs = []
+            for i in range(n):
+                B, d = int(Bs[i]), int(dirs[i])
+                k = slot.get((B, d), 0)
+                slot[(B, d)] = (k + 1) % pool
+                prev = last.get((B, d, k))
+                if prev is not None:
+                    prev.wait(300)                 # the output buffer is free again
+                while time.perf_counter() < due[i]:
+                    pass
+                r = srv.submit(d, B, ins[B][d], outs[B][d][k])
+                last[(B, d, k)] = r
+                reqs.append(r)
+            for r in reqs:
+                r.wait(300)
+            st = srv.stats()
+            sweep.append({"offered_per_s": rate, "requests": n, "transforms_per_s": st["transforms_per_s"],
+                          "p50_ms": st["p50_ms"], "p99_ms": st["p99_ms"], "mean_ms": st["mean_ms"],
+                          "max_ms": st["max_ms"], "mean_batch": st["mean_batch"],
+                          "max_concurrent_batches": st["max_concurrent_batches"], "peak_bytes": st["peak_bytes"]})
+            print(json.dumps({"rate": rate, **sweep[-1]}), file=sys.stderr, flush=True)
+    best = max(x["transforms_per_s"] for x in sweep)
+    line = {
+        "metric": "served DSOFT/iDSOFT transforms/s under Poisson arrivals (best over the sweep)", "value": best,
+        "unit": "transforms/s", "n_gpus": 1, "steps": len(rates), "warmup": 1, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (device generator)",
+        "config": {"workload": "requests 50/50 DSOFT/iDSOFT, B log-uniform over 16..256 on "
+                               f"{list(SERVE_BANDS)} (seed 4), Poisson arrivals", "rates": rates,
+                   "seconds_per_rate": args.seconds, "budget_bytes": budget, "max_batch": 16, "streams": 4,
+                   "output_buffers_per_bandwidth_and_direction": pool},
+        "sweep": sweep,
     }
     print(json.dumps(line), flush=True)
 
@@ -356,6 +462,9 @@ def main():
         return
     if args.workload == "mixed":
         run_mixed(args)
+        return
+    if args.workload == "serve":
+        run_serve_sweep(args)
         return
 
     import numpy as np
