@@ -7,6 +7,9 @@
 //   pfsoft::grid3D<complex<double>>           include/PFSOFTlib_headers/grid3D_cx.hpp:47-83
 //   pfsoft::DSOFTFourierCoefficients          include/PFSOFTlib_headers/dsoft_fourier_coefficients.hpp:50-72
 //   pfsoft::FourierTransforms::DSOFT/IDSOFT   include/PFSOFTlib_headers/fn_fourier_transforms.hpp:75-78
+//   operator<< of complex, grid3D, DSOFTFourierCoefficients
+//                                             complex.hpp:596, grid3D_cx.hpp:429-523,
+//                                             src/dsoft_fourier_coefficients.cpp:124-137
 //
 // Differences a caller can observe: DSOFT takes the sample by const reference (every call site
 // of the by-value original still compiles, and the caller's grid is untouched either way);
@@ -17,10 +20,15 @@
 #define PFSOFT_B200_PFSOFT_HPP
 
 #include <algorithm>
+#include <cmath>
 #include <cstddef>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <iomanip>
+#include <iostream>
+#include <sstream>
+#include <string>
 #include <utility>
 #include <vector>
 
@@ -131,6 +139,109 @@ struct DSOFTFourierCoefficients {
         return (size_t)l * (4 * (size_t)l * l - 1) / 3 + i2 * L + i1;
     }
 };
+
+// ---- text output, in the reference's format ------------------------------------------------
+namespace detail {
+
+// Column layout of the reference's complex grid and matrix printers: width 20 in fixed
+// notation; the LAST element (in print order) whose real or imaginary magnitude reaches 10, 100
+// or 1000 sets the width to 22, 24 or 28, the last of these in scientific notation.
+struct CellFormat {
+    int width = 20;
+    bool scientific = false;
+    void see(double re, double im)
+    {
+        const double a = std::abs(re), b = std::abs(im);
+        if (a >= 10 || b >= 10) {
+            width = 22;
+            scientific = false;
+        }
+        if (a >= 100 || b >= 100) {
+            width = 24;
+            scientific = false;
+        }
+        if (a >= 1000 || b >= 1000) {
+            width = 28;
+            scientific = true;
+        }
+    }
+};
+
+// "re + |im|i" with four decimals; a zero imaginary part prints as +0
+inline std::string cell_text(double re, double im, bool scientific)
+{
+    std::ostringstream v;
+    if (scientific)
+        v << std::scientific;
+    else
+        v << std::fixed;
+    v << std::setprecision(4) << re << (im < 0 ? " - " : " + ") << (im == 0 ? 0.0 : std::abs(im)) << "i";
+    return v.str();
+}
+
+inline void put_cell(std::ostream& o, const CellFormat& f, double re, double im)
+{
+    o << std::setfill(' ') << std::right << std::setw(f.width) << cell_text(re, im, f.scientific);
+}
+
+}  // namespace detail
+
+// complex.hpp:596: scientific, 4 digits; leaves the stream in fixed notation
+template <typename T>
+std::ostream& operator<<(std::ostream& o, const complex<T>& c)
+{
+    const std::ios::fmtflags saved = std::cout.flags();
+    o << std::scientific << std::setprecision(4) << std::noshowpos << c.re << (c.im < 0 ? " - " : " + ")
+      << (c.im == 0 ? 0 : std::abs(c.im)) << "i";
+    std::cout.flags(saved);
+    return o << std::fixed;
+}
+
+// grid3D_cx.hpp:429-523: a blank line, then per layer "layer[z]" and one row per grid row
+template <typename T>
+std::ostream& operator<<(std::ostream& o, const grid3D<complex<T> >& g)
+{
+    const std::ios::fmtflags saved = std::cout.flags();
+    o << std::endl;
+    detail::CellFormat f;
+    for (size_t z = 0; z < g.lays; ++z)
+        for (size_t x = 0; x < g.rows; ++x)
+            for (size_t y = 0; y < g.cols; ++y) f.see((double)g(x, y, z).re, (double)g(x, y, z).im);
+    for (size_t z = 0; z < g.lays; ++z) {
+        o << "layer[" << z << "]" << std::endl;
+        for (size_t x = 0; x < g.rows; ++x) {
+            for (size_t y = 0; y < g.cols; ++y) detail::put_cell(o, f, (double)g(x, y, z).re, (double)g(x, y, z).im);
+            o << std::endl;
+        }
+        o << std::endl;
+    }
+    std::cout.flags(saved);
+    return o;
+}
+
+// src/dsoft_fourier_coefficients.cpp:124-137: per degree a title line and the (2l+1)^2 block,
+// rows = order M, columns = order M' (0, 1, ..., l, -l, ..., -1), in the matrix format above
+inline std::ostream& operator<<(std::ostream& o, const DSOFTFourierCoefficients& fc)
+{
+    const std::ios::fmtflags saved = std::cout.flags();
+    o << std::endl << std::setprecision(4);
+    for (int l = 0; l < fc.bandwidth; ++l) {
+        o << "DSOFTFourierCoefficients[M_{0,1,2,...,-2,-1} x M'_{0,1,2,...,-2,-1}] ~> [l = " << l << "]" << std::endl;
+        const size_t L = 2 * (size_t)l + 1, base = (size_t)l * (4 * (size_t)l * l - 1) / 3;
+        const complex<double>* blk = fc.data() + base;   // column-major: (row i, column j) at j L + i
+        detail::CellFormat f;
+        o << std::endl;
+        for (size_t i = 0; i < L; ++i)
+            for (size_t j = 0; j < L; ++j) f.see(blk[j * L + i].re, blk[j * L + i].im);
+        for (size_t i = 0; i < L; ++i) {
+            for (size_t j = 0; j < L; ++j) detail::put_cell(o, f, blk[j * L + i].re, blk[j * L + i].im);
+            o << std::endl;
+        }
+        o << std::endl;
+    }
+    std::cout.flags(saved);
+    return o;
+}
 
 namespace FourierTransforms {
 

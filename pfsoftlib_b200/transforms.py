@@ -59,6 +59,29 @@ def coef_index(l: int, M: int, Mp: int) -> int:
     return l * (4 * l * l - 1) // 3 + i2 * L + i1
 
 
+def _cell_format(values):
+    """Width and notation of the reference's complex grid / matrix printers (grid3D_cx.hpp:429-523,
+    matrix_cx.hpp:545-620): 20, fixed; the last value in print order whose real or imaginary
+    magnitude reaches 10, 100 or 1000 sets 22, 24 or 28 (the last in scientific notation)."""
+    width, sci = 20, False
+    for v in values:
+        a, b = abs(v.real), abs(v.imag)
+        if a >= 10 or b >= 10:
+            width, sci = 22, False
+        if a >= 100 or b >= 100:
+            width, sci = 24, False
+        if a >= 1000 or b >= 1000:
+            width, sci = 28, True
+    return width, sci
+
+
+def _cell(v, width, sci):
+    f = "%.4e" if sci else "%.4f"
+    im = v.imag
+    text = (f % v.real) + (" - " if im < 0 else " + ") + (f % (0.0 if im == 0 else abs(im))) + "i"
+    return text.rjust(width)
+
+
 class grid3D:
     """Complex (2B)^3 sample grid, element (row, col, lay) at (lay*cols + col)*rows + row.
 
@@ -104,6 +127,20 @@ class grid3D:
 
     def copy(self) -> "grid3D":
         return grid3D.wrap(self.mem.clone() if _is_torch(self.mem) else self.mem.copy())
+
+    def __str__(self) -> str:
+        """The reference's ``operator<<`` text (grid3D_cx.hpp:429-523): a blank line, then per
+        layer ``layer[z]`` and one line per grid row."""
+        m = self.mem.cpu().numpy() if _is_torch(self.mem) else np.asarray(self.mem)
+        order = [complex(m[z, y, x]) for z in range(self.lays) for x in range(self.rows) for y in range(self.cols)]
+        width, sci = _cell_format(order)
+        out = ["\n"]
+        for z in range(self.lays):
+            out.append(f"layer[{z}]\n")
+            for x in range(self.rows):
+                out.append("".join(_cell(complex(m[z, y, x]), width, sci) for y in range(self.cols)) + "\n")
+            out.append("\n")
+        return "".join(out)
 
     def _layer_wise(self, scale: complex, inverse: bool):
         if not self.on_device:
@@ -167,6 +204,21 @@ class DSOFTFourierCoefficients:
 
     def __setitem__(self, idx, value):
         self.mem[self._index(*idx)] = value
+
+    def __str__(self) -> str:
+        """The reference's ``operator<<`` text (src/dsoft_fourier_coefficients.cpp:124-137): per
+        degree a title line and the (2l+1)^2 block, rows = M, columns = M'."""
+        m = self.mem.cpu().numpy() if _is_torch(self.mem) else np.asarray(self.mem)
+        out = ["\n"]
+        for l in range(self.bandwidth):
+            out.append(f"DSOFTFourierCoefficients[M_{{0,1,2,...,-2,-1}} x M'_{{0,1,2,...,-2,-1}}] ~> [l = {l}]\n\n")
+            L, base = 2 * l + 1, l * (4 * l * l - 1) // 3
+            blk = m[base:base + L * L].reshape(L, L)   # [column M'][row M]
+            width, sci = _cell_format(complex(blk[j, i]) for i in range(L) for j in range(L))
+            for i in range(L):
+                out.append("".join(_cell(complex(blk[j, i]), width, sci) for j in range(L)) + "\n")
+            out.append("\n")
+        return "".join(out)
 
 
 class FourierTransforms:
