@@ -349,14 +349,32 @@ __global__ void __launch_bounds__(kWarps * 32, CS == 2 ? 3 : 1)
                 bv1[n] = gb[4 * 16 + v];
             }
             auto mma_step = [&](int s) {
+                // subtiles spread over the 8 steps; the two k-halves of an accumulator are issued
+                // a full round apart so that dependent MMAs do not follow each other
+                constexpr int PS = (NSUB8 + 7) / 8;
+                double av0[PS], av1[PS];
 #pragma unroll
-                for (int p = s; p < NSUB8; p += 8) {   // subtiles spread over the 8 steps
-                    const double av0 = dc[t4 * DS + 8 * p + g];
-                    const double av1 = dc[(4 + t4) * DS + 8 * p + g];
+                for (int i = 0; i < PS; ++i) {
+                    const int p = s + 8 * i;
+                    if (p < NSUB8) {
+                        av0[i] = dc[t4 * DS + 8 * p + g];
+                        av1[i] = dc[(4 + t4) * DS + 8 * p + g];
+                    }
+                }
 #pragma unroll
-                    for (int n = 0; n < NT; ++n) {
-                        dmma(acc[p][n][0], acc[p][n][1], av0, bv0[n]);
-                        dmma(acc[p][n][0], acc[p][n][1], av1, bv1[n]);
+                for (int i = 0; i < PS; ++i) {
+                    const int p = s + 8 * i;
+                    if (p < NSUB8) {
+#pragma unroll
+                        for (int n = 0; n < NT; ++n) dmma(acc[p][n][0], acc[p][n][1], av0[i], bv0[n]);
+                    }
+                }
+#pragma unroll
+                for (int i = 0; i < PS; ++i) {
+                    const int p = s + 8 * i;
+                    if (p < NSUB8) {
+#pragma unroll
+                        for (int n = 0; n < NT; ++n) dmma(acc[p][n][0], acc[p][n][1], av1[i], bv1[n]);
                     }
                 }
             };

@@ -238,13 +238,14 @@ __global__ void __launch_bounds__(64 * TT) dwt_batch_kernel(const DwtGroup* __re
                         const double bv0 = gt[(b0 + t4) * L::GS], bv1 = gt[(b0 + 4 + t4) * L::GS];
                         const double* d0 = s_d + (b0 + t4) * DS + g;
                         const double* d1 = s_d + (b0 + 4 + t4) * DS + g;
+                        // narrower bandwidths in a wider launch skip empty tiles; the two k-halves
+                        // of an accumulator are issued a full round apart
 #pragma unroll
-                        for (int p = 0; p < NSUB8; ++p) {
-                            if (8 * p < N) {   // narrower bandwidths in a wider launch skip empty tiles
-                                dmma(acc[p][0], acc[p][1], d0[8 * p], bv0);
-                                dmma(acc[p][0], acc[p][1], d1[8 * p], bv1);
-                            }
-                        }
+                        for (int p = 0; p < NSUB8; ++p)
+                            if (8 * p < N) dmma(acc[p][0], acc[p][1], d0[8 * p], bv0);
+#pragma unroll
+                        for (int p = 0; p < NSUB8; ++p)
+                            if (8 * p < N) dmma(acc[p][0], acc[p][1], d1[8 * p], bv1);
                     }
                 }
                 __syncthreads();   // tile and coefficient chunk are rewritten by the next chunk
