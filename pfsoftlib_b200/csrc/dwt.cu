@@ -55,6 +55,12 @@ struct InvSmem {
     static constexpr size_t doubles = g_off + (size_t)kWarps * 2 * kLB * 16;
 };
 
+// CTAs per SM the register budget is cut for (measured on B200 at B = 128: the 2-column, 4-warp
+// teams gain 12-16 % over 255-register, 2-CTA kernels at 3-4 CTAs per SM; the inverse spills
+// past 3).
+constexpr int fwd_min_blocks(int KT, int TW, int CS) { return KT == 2 && TW == 4 ? 4 : (CS == 2 ? 4 : 1); }
+constexpr int inv_min_blocks(int KT, int TW, int CS) { return KT == 2 && TW == 4 ? 3 : (CS == 2 ? 3 : 1); }
+
 // Team layout shared by both directions: TW column warps x CS case warps. Warp `wt` of the team
 // owns beta columns [cw*KW, cw*KW + KW) (cw = wt / CS) and, with CS = 2, only the four cases
 // 4h .. 4h+3 (h = wt % CS, one MMA n-tile); the pair of case warps runs the same recurrence
@@ -82,7 +88,7 @@ struct Team {
 // Forward DWT (see the header comment). The rows of 8-degree block b+1 are generated while
 // block b is contracted (two row buffers).
 template <int KT, int TW, int CS>
-__global__ void __launch_bounds__(kWarps * 32, CS == 2 ? 4 : 1)
+__global__ void __launch_bounds__(kWarps * 32, fwd_min_blocks(KT, TW, CS))
     dwt_forward_kernel(const double2* __restrict__ X, double* __restrict__ out, const DwtArgs a)
 {
     using L = FwdSmem<KT>;
@@ -251,7 +257,7 @@ __global__ void __launch_bounds__(kWarps * 32, CS == 2 ? 4 : 1)
 // applied (two MMA k-steps of 4 degrees). Coefficients move through registers one 32-degree
 // chunk ahead of their use; the first chunk of the next class is fetched during this one.
 template <int KT, int TW, int CS>
-__global__ void __launch_bounds__(kWarps * 32, CS == 2 ? 3 : 1)
+__global__ void __launch_bounds__(kWarps * 32, inv_min_blocks(KT, TW, CS))
     dwt_inverse_kernel(const double2* __restrict__ coeffs, double2* __restrict__ X, const DwtArgs a)
 {
     using L = InvSmem<KT>;
@@ -484,7 +490,6 @@ cudaError_t launch_inv(const double2* coeffs, double2* X, const DwtArgs& a, int 
 int dwt_team_warps(int N)
 {
     if (N <= 128) return 1;
-    if (N <= 256) return 2;
     return 4;
 }
 
@@ -500,7 +505,7 @@ cudaError_t dwt_forward_launch(const double2* X, double2* coeffs, const DwtArgs&
     if (N <= 32) return launch_fwd<1, 1, 1>(X, coeffs, a, nblocks, s);
     if (N <= 64) return launch_fwd<2, 1, 1>(X, coeffs, a, nblocks, s);
     if (N <= 128) return split ? launch_fwd<4, 1, 2>(X, coeffs, a, nblocks, s) : launch_fwd<4, 1, 1>(X, coeffs, a, nblocks, s);
-    if (N <= 256) return split ? launch_fwd<4, 2, 2>(X, coeffs, a, nblocks, s) : launch_fwd<4, 2, 1>(X, coeffs, a, nblocks, s);
+    if (N <= 256) return split ? launch_fwd<4, 2, 2>(X, coeffs, a, nblocks, s) : launch_fwd<2, 4, 1>(X, coeffs, a, nblocks, s);
     if (N <= 512) return split ? launch_fwd<8, 2, 2>(X, coeffs, a, nblocks, s) : launch_fwd<4, 4, 1>(X, coeffs, a, nblocks, s);
     return cudaErrorInvalidValue;
 }
@@ -512,7 +517,7 @@ cudaError_t dwt_inverse_launch(const double2* coeffs, double2* X, const DwtArgs&
     if (N <= 32) return launch_inv<1, 1, 1>(coeffs, X, a, nblocks, s);
     if (N <= 64) return launch_inv<2, 1, 1>(coeffs, X, a, nblocks, s);
     if (N <= 128) return split ? launch_inv<4, 1, 2>(coeffs, X, a, nblocks, s) : launch_inv<4, 1, 1>(coeffs, X, a, nblocks, s);
-    if (N <= 256) return split ? launch_inv<4, 2, 2>(coeffs, X, a, nblocks, s) : launch_inv<4, 2, 1>(coeffs, X, a, nblocks, s);
+    if (N <= 256) return split ? launch_inv<4, 2, 2>(coeffs, X, a, nblocks, s) : launch_inv<2, 4, 1>(coeffs, X, a, nblocks, s);
     if (N <= 512) return split ? launch_inv<8, 2, 2>(coeffs, X, a, nblocks, s) : launch_inv<4, 4, 1>(coeffs, X, a, nblocks, s);
     return cudaErrorInvalidValue;
 }
