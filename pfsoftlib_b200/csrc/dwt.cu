@@ -45,14 +45,17 @@ struct FwdSmem {
     static constexpr size_t doubles = red_off + (size_t)2 * kWarps * 8 * 16;
 };
 
-template <int KT>
+template <int KT, int TEAMS>
 struct InvSmem {
     static constexpr int KW = 32 * KT;
     static constexpr int DS = KW + 8;   // padded row stride for the transposed A-fragment loads
+    // coefficient row stride: with one team per CTA 16 values + 4, so that the B-fragment loads of
+    // the four t4 rows hit distinct banks; with four teams 16, which keeps two CTAs per SM
+    static constexpr int GS = TEAMS == 1 ? 20 : 16;
     static constexpr size_t d_off = 0;                                       // [kWarps][2][8][DS]
     static constexpr size_t rc_off = d_off + (size_t)kWarps * 2 * 8 * DS;     // [kWarps][kLB][4]
-    static constexpr size_t g_off = rc_off + (size_t)kWarps * kLB * 4;       // [teams][2][kLB][16]
-    static constexpr size_t doubles = g_off + (size_t)kWarps * 2 * kLB * 16;
+    static constexpr size_t g_off = rc_off + (size_t)kWarps * kLB * 4;       // [TEAMS][2][kLB][GS]
+    static constexpr size_t doubles = g_off + (size_t)TEAMS * 2 * kLB * GS;
 };
 
 // CTAs per SM the register budget is cut for (measured on B200 at B = 128: the 2-column, 4-warp
@@ -260,7 +263,7 @@ template <int KT, int TW, int CS>
 __global__ void __launch_bounds__(kWarps * 32, inv_min_blocks(KT, TW, CS))
     dwt_inverse_kernel(const double2* __restrict__ coeffs, double2* __restrict__ X, const DwtArgs a)
 {
-    using L = InvSmem<KT>;
+    using L = InvSmem<KT, kWarps / (TW * CS)>;
     using TM = Team<KT, TW, CS>;
     constexpr int KW = L::KW, DS = L::DS, NSUB8 = KW / 8;
     constexpr int NT = TM::NT;
@@ -271,7 +274,11 @@ __global__ void __launch_bounds__(kWarps * 32, inv_min_blocks(KT, TW, CS))
     const int lane = tm.lane, g = tm.g, t4 = tm.t4;
     double* s_d = smem + L::d_off + (size_t)tm.warp * 2 * 8 * DS;
     double* s_rc = smem + L::rc_off + (size_t)tm.warp * kLB * 4;
-    double* s_g = smem + L::g_off + (size_t)tm.team * 2 * kLB * 16;   // [2][kLB][16]
+    constexpr int GS = L::GS;
+    // one team per CTA: consecutive lanes stage the cases of one degree (one contiguous row, no
+    // bank conflicts); four one-warp teams measured faster with consecutive degrees per lane
+    constexpr bool kCaseFirst = kWarps / (TW * CS) == 1;
+    double* s_g = smem + L::g_off + (size_t)tm.team * 2 * kLB * GS;   // [2][kLB][GS]
     const int B = a.B, N = a.N;
     const int ncls = num_classes(B);
     const double norm = (double)(B * 2 * B) / kPi;   // src/fn_idsoft.cpp:109
@@ -290,7 +297,8 @@ __global__ void __launch_bounds__(kWarps * 32, inv_min_blocks(KT, TW, CS))
         const int nc = class_case_count(M, Mp);
 #pragma unroll
         for (int i = 0; i < PER; ++i) {
-            const int e = tm.tl + i * TT, c = e / kLB, ld = l + (e - c * kLB);
+            const int e = tm.tl + i * TT;
+            const int c = kCaseFirst ? (e & 7) : e / kLB, ld = l + (kCaseFirst ? (e >> 3) : e % kLB);
             double2 v = make_double2(0.0, 0.0);
             if (e < 8 * kLB && c < nc && ld < B) {
                 const PairCase p = class_case(M, Mp, c, N);
@@ -304,8 +312,9 @@ __global__ void __launch_bounds__(kWarps * 32, inv_min_blocks(KT, TW, CS))
     auto stash = [&](int buf) {
 #pragma unroll
         for (int i = 0; i < PER; ++i) {
-            const int e = tm.tl + i * TT, c = e / kLB, j = e - c * kLB;
-            if (e < 8 * kLB) *reinterpret_cast<double2*>(s_g + (buf * kLB + j) * 16 + 2 * c) = pf[i];
+            const int e = tm.tl + i * TT;
+            const int c = kCaseFirst ? (e & 7) : e / kLB, j = kCaseFirst ? (e >> 3) : e % kLB;
+            if (e < 8 * kLB) *reinterpret_cast<double2*>(s_g + (buf * kLB + j) * GS + 2 * c) = pf[i];
         }
     };
 
@@ -346,13 +355,13 @@ __global__ void __launch_bounds__(kWarps * 32, inv_min_blocks(KT, TW, CS))
             const double* dc = s_d + cur * 8 * DS;
             double* dn = s_d + (cur ^ 1) * 8 * DS;
             // B fragments for the two k-steps (degrees off + t4 and off + 4 + t4)
-            const double* gb = s_g + ((((off >> 5) & 1) * kLB) + (off & (kLB - 1)) + t4) * 16;
+            const double* gb = s_g + ((((off >> 5) & 1) * kLB) + (off & (kLB - 1)) + t4) * GS;
             double bv0[NT], bv1[NT];
 #pragma unroll
             for (int n = 0; n < NT; ++n) {
                 const int v = 8 * (CS == 2 ? tm.h : n) + g;
                 bv0[n] = gb[v];
-                bv1[n] = gb[4 * 16 + v];
+                bv1[n] = gb[4 * GS + v];
             }
             auto mma_step = [&](int s) {
                 // subtiles spread over the 8 steps; the two k-halves of an accumulator are issued
@@ -476,7 +485,7 @@ cudaError_t launch_fwd(const double2* X, double2* coeffs, const DwtArgs& a, int 
 template <int KT, int TW, int CS>
 cudaError_t launch_inv(const double2* coeffs, double2* X, const DwtArgs& a, int nblocks, cudaStream_t s)
 {
-    const size_t smem = InvSmem<KT>::doubles * sizeof(double);
+    const size_t smem = InvSmem<KT, kWarps / (TW * CS)>::doubles * sizeof(double);
     auto k = dwt_inverse_kernel<KT, TW, CS>;
     cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
