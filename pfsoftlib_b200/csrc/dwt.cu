@@ -144,6 +144,8 @@ __global__ void __launch_bounds__(kWarps * 32, fwd_min_blocks(KT, TW, CS))
             }
             po[n] = class_case(M, Mp, 4 * nn + t4 < nc ? 4 * nn + t4 : 0, N);
         }
+        // the case this thread sums in the cross-warp reduction (tl & 7), fixed for the class
+        const PairCase pred = class_case(M, Mp, (tm.tl & 7) < nc ? (tm.tl & 7) : 0, N);
 
         {
             // the next class's beta columns (this warp's slice) into L2 while this one runs
@@ -242,9 +244,8 @@ __global__ void __launch_bounds__(kWarps * 32, fwd_min_blocks(KT, TW, CS))
                             sum.x += v.x;
                             sum.y += v.y;
                         }
-                        const PairCase p = class_case(M, Mp, c, N);
-                        const double f = norm * case_sign(p, l, M);
-                        *reinterpret_cast<double2*>(out + 2 * coef_index(l, p.m1, p.m2)) = make_double2(f * sum.x, f * sum.y);
+                        const double f = norm * case_sign(pred, l, M);   // c == tl & 7
+                        *reinterpret_cast<double2*>(out + 2 * coef_index(l, pred.m1, pred.m2)) = make_double2(f * sum.x, f * sum.y);
                     }
                 }
                 redbuf ^= 1;
