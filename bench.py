@@ -570,7 +570,7 @@ def main():
     d = stages[dominant]
     # DRAM bytes per launch (read + write) from one ncu capture of the same kernels at B = 128,
     # profiles/dwt_single_b128.md and profiles/fft_pass_b128.md
-    traffic = {"dwt_forward": 268.34e6 + 45.13e6, "dwt_inverse": 46.49e6 + 209.40e6,
+    traffic = {"dwt_forward": 268.37e6 + 43.51e6, "dwt_inverse": 46.44e6 + 208.20e6,
                "fft_forward_gamma": 268.5e6 + 221.6e6, "fft_inverse_alpha": 268.5e6 + 214.7e6,
                "fft_inverse_gamma": 268.5e6 + 219.7e6}
     roofline = {"kernel": dominant, "bound": d["bound"], "achieved": d["achieved"], "peak": d["peak"],
