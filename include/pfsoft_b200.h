@@ -171,7 +171,9 @@ int pfsoft_cuda_random_coeffs(double* d_coeffs, int B, unsigned long long seed, 
  *   PFSOFT_EBUSY if it is already on the GPU.
  * pause(1) stops new launches (queued requests keep accumulating); pause(0) resumes.
  * drain: waits until nothing is queued or running (PFSOFT_ETIMEOUT after timeout_s).
- * destroy: cancels what is queued, waits for what runs, frees everything. */
+ * destroy: cancels what is queued, waits for what runs, frees everything; no other call on the
+ *   same server may run concurrently with it or follow it. Other calls are thread-safe.
+ * Latency statistics cover the most recent 2^20 completed requests since the last reset. */
 typedef struct pfsoft_server pfsoft_server;
 typedef struct pfsoft_server_stats {
     long long submitted, completed, cancelled, rejected, failed;

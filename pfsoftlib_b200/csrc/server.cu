@@ -48,6 +48,7 @@ namespace {
 constexpr size_t kStageHeader = 128;   // DwtGroup, padded; pointer tables follow
 constexpr int kMaxBatchLimit = 256;
 constexpr int kMaxStreams = 16;
+constexpr size_t kLatencyWindow = (size_t)1 << 20;   // latency samples kept (the most recent)
 
 double now_s()
 {
@@ -121,7 +122,8 @@ struct pfsoft_server {
     std::thread worker;
     // statistics since the last reset
     long long submitted = 0, completed = 0, cancelled = 0, rejected = 0, failed = 0, batches = 0, batched = 0;
-    std::vector<double> lat_ms;
+    std::vector<double> lat_ms;   // ring of the last kLatencyWindow latencies
+    size_t lat_next = 0;
     double t_first = -1, t_last = 0;
     int max_concurrent = 0;
 };
@@ -230,7 +232,12 @@ void finish_batch(pfsoft_server* s, Batch* b, double t_done, int status)
         r.t_done = t_done;
         if (status == PFSOFT_OK) {
             ++s->completed;
-            s->lat_ms.push_back((t_done - r.t_submit) * 1e3);
+            const double ms = (t_done - r.t_submit) * 1e3;
+            if (s->lat_ms.size() < kLatencyWindow)
+                s->lat_ms.push_back(ms);
+            else
+                s->lat_ms[s->lat_next] = ms;
+            s->lat_next = (s->lat_next + 1) % kLatencyWindow;
             s->t_last = std::max(s->t_last, t_done);
         } else {
             ++s->failed;
@@ -554,6 +561,7 @@ int pfsoft_server_reset_stats(pfsoft_server* s)
     std::lock_guard<std::mutex> lk(s->mu);
     s->submitted = s->completed = s->cancelled = s->rejected = s->failed = s->batches = s->batched = 0;
     s->lat_ms.clear();
+    s->lat_next = 0;
     s->t_first = -1;
     s->t_last = 0;
     s->max_concurrent = s->running;

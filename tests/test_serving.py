@@ -79,12 +79,12 @@ def _rel(a, b):
     return ((a - b).abs().pow(2).sum().sqrt() / b.abs().pow(2).sum().sqrt()).item()
 
 
-def _mix(lib, torch, n=24, seed=5):
-    """n requests: bandwidths over {4, 8, 16, 24, 32, 48, 64}, both directions, plain results."""
+def _mix(lib, torch, n=28, seed=5):
+    """n requests: bandwidths over {1, 2, 3, 5, 8, 16, 24, 32, 48, 64}, both directions, plain results."""
     rng = np.random.default_rng(seed)
     out = []
     for i in range(n):
-        B = int(rng.choice((4, 8, 16, 24, 32, 48, 64)))
+        B = int(rng.choice((1, 2, 3, 5, 8, 16, 24, 32, 48, 64)))
         direction = int(rng.integers(0, 2))
         c = _coeffs(lib, torch, B, 100 + i)
         inp = c if direction == 1 else _plain(lib, torch, 1, B, c)
