@@ -46,7 +46,6 @@ int cuda_fail(cudaError_t e, const char* what)
     } while (0)
 
 constexpr int kMaxBandwidth = 512;
-constexpr int kFftKB = 8;   // vectors per FFT tile: 8 complex128 = 128 contiguous bytes
 
 struct DeviceState {
     std::mutex mu;
@@ -204,7 +203,7 @@ FftPassArgs pass_args(int n, int nvec, const BandTables& t, FftStrides src, FftS
     memset(&a, 0, sizeof(a));   // srcs/dsts null: single transform
     a.n = n;
     a.nvec = nvec;
-    a.kb = kFftKB;
+    a.kb = fft_tile_vectors(n);
     a.nstages = fft_plan_radices(n, a.radix, a.ns);
     a.src = src;
     a.dst = dst;
@@ -523,7 +522,7 @@ static int layer_wise(int cols, int rows, int lays, double* d_arr, double scale,
         FftPassArgs a;
         memset(&a, 0, sizeof(a));
         a.n = n;
-        a.kb = kFftKB;
+        a.kb = fft_tile_vectors(n);
         a.nstages = fft_plan_radices(n, a.radix, a.ns);
         a.twiddle = tw;
         a.scale = pass == 1 ? scale : 1.0;

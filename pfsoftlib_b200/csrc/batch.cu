@@ -76,7 +76,7 @@ FftPassArgs group_pass_args(int dir, bool first, const BandTables& t, double2** 
     memset(&a, 0, sizeof(a));
     a.n = t.N;
     a.nvec = t.N;
-    a.kb = 8;
+    a.kb = fft_tile_vectors(t.N);
     a.nstages = fft_plan_radices(t.N, a.radix, a.ns);
     a.twiddle = t.twiddle;
     a.scale = 1.0;

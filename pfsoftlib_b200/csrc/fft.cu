@@ -321,6 +321,12 @@ int fft_plan_radices(int n, int* radix, int* ns)
     return cnt;
 }
 
+int fft_tile_vectors(int n)
+{
+    const size_t two_buffers = 2 * (size_t)8 * padded_len(n) * sizeof(double2);
+    return two_buffers > (size_t)110 * 1024 ? 4 : 8;
+}
+
 size_t fft_pass_smem_bytes(const FftPassArgs& a)
 {
     const int buffers = a.nstages >= 3 ? 2 : (a.nstages == 2 ? 1 : 0);

@@ -40,4 +40,8 @@ cudaError_t fft_pass_launch(const double2* src, double2* dst, const FftPassArgs&
 
 size_t fft_pass_smem_bytes(const FftPassArgs& a);
 
+// Vectors per tile for length n: 8 (128 contiguous bytes on the transposed side) unless the
+// ping-pong buffers of 8 vectors would leave a single CTA per SM (long transforms, n = 512), then 4.
+int fft_tile_vectors(int n);
+
 }  // namespace pfsoft_dev

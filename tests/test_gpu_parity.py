@@ -132,7 +132,8 @@ def test_host_staged_matches_device(lib):
     np.testing.assert_array_equal(f_host, gpu_dsoft(lib, g_host, B)[0])
 
 
-@pytest.mark.parametrize("cols,rows,lays", [(8, 8, 3), (32, 32, 5), (24, 40, 2), (7, 9, 3), (256, 256, 2), (512, 512, 1)])
+@pytest.mark.parametrize("cols,rows,lays", [(8, 8, 3), (32, 32, 5), (24, 40, 2), (7, 9, 3), (256, 256, 2), (512, 512, 1),
+                                             (512, 384, 5), (384, 512, 6)])
 def test_layer_wise_fft_matches_numpy(lib, cols, rows, lays):
     rng = np.random.default_rng(cols * rows)
     x = rng.standard_normal((lays, cols, rows)) + 1j * rng.standard_normal((lays, cols, rows))
@@ -175,3 +176,17 @@ def test_wigner_matrix_large_orders_match_oracle(lib, oracle):
         d = out.cpu().numpy().reshape(B - J, 2 * B)
         ref = oracle.wigner_d(B, M, Mp)
         assert np.abs(d - ref).max() <= 1e-12 * max(1.0, np.abs(ref).max())
+
+
+def test_round_trip_b256(lib):
+    """B = 256 (512^3 grid: the FFT passes run 4-vector tiles): IDSOFT then DSOFT."""
+    B = 256
+    s = stream()
+    c = torch.empty(B * (4 * B * B - 1) // 3, dtype=torch.complex128, device="cuda")
+    assert lib.pfsoft_cuda_random_coeffs(c.data_ptr(), B, 11, 2, 1.0, s) == 0
+    g = torch.empty((2 * B,) * 3, dtype=torch.complex128, device="cuda")
+    f = torch.empty_like(c)
+    assert lib.pfsoft_cuda_idsoft(c.data_ptr(), B, g.data_ptr(), None, 0, s) == 0
+    assert lib.pfsoft_cuda_dsoft(g.data_ptr(), B, f.data_ptr(), None, 0, s) == 0
+    torch.cuda.synchronize()
+    assert (torch.linalg.vector_norm(f - c) / torch.linalg.vector_norm(c)).item() <= 1e-13
