@@ -38,9 +38,9 @@ TRANSFORMS_PER_STEP = 2
 GRID_BYTES = N ** 3 * 16
 COEF_COUNT = B * (4 * B * B - 1) // 3
 COEF_BYTES = COEF_COUNT * 16
-FP64_PEAK_TFLOPS = 37.0   # mma.sync m8n8k4 f64 on this pool's B200 (DFMA measured 33.5)
+FP64_PEAK_TFLOPS = 37.0   # mma.sync m8n8k4 f64 measured on B200 (DFMA 33.5), pfsoftlib_b200/peaks
 
-# algorithmic work per transform (see DESIGN.md "Roofline"):
+# algorithmic work per transform:
 #   each FFT pass reads and writes the grid once: 32 N^3 bytes
 #   each DWT does 8 B^2 (4B^2-1)/3 useful FP64 flops
 FFT_PASS_BYTES = 2 * GRID_BYTES

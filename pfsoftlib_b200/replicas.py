@@ -3,7 +3,7 @@ no collective touches the data path. Only the timing uses a collective (max over
 
 The work of one transform at bandwidth B is dominated by the discrete Wigner transform,
 ~8 B^2 (4B^2-1)/3 FP64 flops, plus 5 passes of 16 (2B)^3 bytes over HBM; ``transform_cost``
-weighs both with this pool's measured peaks so that ranks receive equal device time.
+weighs both with measured B200 peaks so that ranks receive equal device time.
 """
 from __future__ import annotations
 
