@@ -87,3 +87,42 @@ def test_batch_rejects_bad_arguments(lib):
     assert lib.pfsoft_batch_create(arr, 2, 0, 0, ctypes.byref(plan)) == 1
     arr = (ctypes.c_int * 1)(8)
     assert lib.pfsoft_batch_create(arr, 1, 3, 0, ctypes.byref(plan)) == 1
+
+
+def test_python_batch_plan(lib):
+    """pfsoftlib_b200.BatchPlan: same results as the single-transform entry points, split mode
+    within 1e-11, argument checks raise before any launch."""
+    import torch
+
+    from pfsoftlib_b200 import BatchPlan, PfsoftError
+
+    bws = [16, 8, 16, 32, 5]
+    s = torch.cuda.current_stream().cuda_stream
+    cs = []
+    for i, B in enumerate(bws):
+        c = torch.empty(B * (4 * B * B - 1) // 3, dtype=torch.complex128, device="cuda")
+        assert lib.pfsoft_cuda_random_coeffs(c.data_ptr(), B, 40 + i, 1, 1.0, s) == 0
+        cs.append(c)
+    grids = [torch.empty((2 * B,) * 3, dtype=torch.complex128, device="cuda") for B in bws]
+    back = [torch.empty_like(c) for c in cs]
+    with BatchPlan(bws) as plan:
+        assert plan.transforms_per_cta in (1, 2, 4) and plan.workspace_bytes > 0
+        plan.idsoft(cs, grids)
+        plan.dsoft(grids, back)
+    for B, c, g, f in zip(bws, cs, grids, back):
+        assert orc.rel_l2(g.cpu().numpy(), _single(lib, "idsoft", c, B).cpu().numpy()) <= REL_TOL
+        assert orc.rel_l2(f.cpu().numpy(), _single(lib, "dsoft", g, B).cpu().numpy()) <= REL_TOL
+    with BatchPlan(bws, split=True) as plan:
+        sg = [torch.empty_like(g) for g in grids]
+        plan.idsoft(cs, sg)
+        plan.status()
+    for g, h in zip(grids, sg):
+        assert (torch.linalg.vector_norm(h - g) / torch.linalg.vector_norm(g)).item() <= 1e-11
+    plan = BatchPlan([8, 8])
+    with pytest.raises(ValueError):
+        plan.dsoft(grids[:2], back[:2])           # sizes do not match B = 8
+    with pytest.raises(ValueError):
+        plan.dsoft(grids[:1], back[:1])           # wrong count
+    with pytest.raises(PfsoftError):
+        BatchPlan([0])
+    plan.close()
