@@ -198,6 +198,59 @@ int pfsoft_server_drain(pfsoft_server* srv, double timeout_s);
 int pfsoft_server_get_stats(pfsoft_server* srv, pfsoft_server_stats* out);
 int pfsoft_server_reset_stats(pfsoft_server* srv);
 
+/* ---- One transform sharded over several GPUs (no counterpart in the reference) -------------
+ * The reference parallelises one transform over the order classes with OpenMP
+ * (src/fn_dsoft.cpp:134-214, src/fn_idsoft.cpp:124-211) and runs the layer-wise FFT over every beta
+ * layer (src/fftw_wrapper.cpp:47-173). A shard plan splits both over nranks GPUs: rank r owns
+ * the beta layers [first, first + count) of the (2B)^3 grid (pfsoft_shard_layers; grid index
+ * beta outermost, so a slab is one contiguous block of count (2B)^2 values) and a set of order
+ * classes balanced by their work. One exchange moves the FFT bins between the two stages.
+ *
+ * Buffers (complex128, as pairs of doubles; N = 2B; nk = this rank's layer count):
+ *   slab grid        nk * N * N      this rank's layers of the grid
+ *   slab spectrum    nk * N * N      workspace of the FFT passes (bin-major, beta innermost)
+ *   spectrum         N * N * N       workspace of the DWT (only this rank's bins are used)
+ *   coefficients     pfsoft_coef_count(B)
+ *   send / receive   sums of pfsoft_shard_counts (parts by peer rank, in rank order)
+ * DSOFT:  fft_forward(slab grid -> slab spectrum)
+ *         exchange FORWARD (slab spectrum -> every rank's spectrum)
+ *         dwt_forward(spectrum -> coefficients): this rank's classes, zero elsewhere, so the
+ *         element-wise sum over ranks (an all-reduce) is the DSOFT of the whole grid.
+ * iDSOFT: dwt_inverse(coefficients -> spectrum): every rank holds the whole coefficient vector
+ *         and computes its classes' bins
+ *         exchange INVERSE (spectrum -> every rank's slab spectrum)
+ *         fft_inverse(slab spectrum -> slab grid); the slab spectrum is overwritten.
+ * The exchange is either
+ *   scatter: direct stores into each rank's destination buffer; d_dst holds nranks device
+ *            pointers (peer mappings for other GPUs, e.g. symmetric memory or CUDA IPC; a rank
+ *            that receives nothing may be NULL). All ranks' scatters must be complete before
+ *            any rank's next step: the caller synchronises the ranks in between.
+ *   pack, all-to-all, unpack: pack into this rank's send buffer, move it with the caller's
+ *            all-to-all (NCCL), unpack from the receive buffer.
+ * Device tables are made on the first call that takes a stream, on the current device; a plan
+ * serves one device. pfsoft_shard_classes / _bins / _counts / _runs are host-only queries (the
+ * classes and bins of a rank, the values sent to and received from each peer, and the copy runs
+ * of an exchange step: step 0 scatter, 1 pack, 2 unpack; a run copies len values from
+ * src + src_off to buffer `slot` + dst_off). */
+#define PFSOFT_SHARD_FORWARD 0
+#define PFSOFT_SHARD_INVERSE 1
+typedef struct pfsoft_shard_plan pfsoft_shard_plan;
+int pfsoft_shard_create(int B, int nranks, int rank, pfsoft_shard_plan** out);
+void pfsoft_shard_destroy(pfsoft_shard_plan* plan);
+int pfsoft_shard_layers(const pfsoft_shard_plan* plan, int rank, int* first, int* count);
+int pfsoft_shard_classes(const pfsoft_shard_plan* plan, int rank, int* out, int capacity);
+long long pfsoft_shard_bins(const pfsoft_shard_plan* plan, int rank, int* out, long long capacity);
+int pfsoft_shard_counts(const pfsoft_shard_plan* plan, int direction, long long* send, long long* recv);
+long long pfsoft_shard_runs(pfsoft_shard_plan* plan, int direction, int step, long long* src_off, long long* dst_off,
+                            int* slot, int* len, long long capacity);
+int pfsoft_shard_fft_forward(pfsoft_shard_plan* plan, const double* d_slab_grid, double* d_slab_spectrum, void* stream);
+int pfsoft_shard_dwt_forward(pfsoft_shard_plan* plan, const double* d_spectrum, double* d_coeffs, void* stream);
+int pfsoft_shard_dwt_inverse(pfsoft_shard_plan* plan, const double* d_coeffs, double* d_spectrum, void* stream);
+int pfsoft_shard_fft_inverse(pfsoft_shard_plan* plan, double* d_slab_spectrum, double* d_slab_grid, void* stream);
+int pfsoft_shard_scatter(pfsoft_shard_plan* plan, int direction, const double* d_src, double* const* d_dst, void* stream);
+int pfsoft_shard_pack(pfsoft_shard_plan* plan, int direction, const double* d_src, double* d_send, void* stream);
+int pfsoft_shard_unpack(pfsoft_shard_plan* plan, int direction, const double* d_recv, double* d_dst, void* stream);
+
 /* ---- Diagnostics (no counterpart in the reference) -----------------------------------------
  * pfsoft_launch_count: number of CUDA kernels this library has launched in the process.
  * pfsoft_profile_enable(1) brackets every stage the library launches with CUDA events on the

@@ -56,6 +56,20 @@ SIGNATURES = {
     "pfsoft_server_drain": (_c_int, [_vp, _c_double]),
     "pfsoft_server_get_stats": (_c_int, [_vp, _vp]),
     "pfsoft_server_reset_stats": (_c_int, [_vp]),
+    "pfsoft_shard_create": (_c_int, [_c_int, _c_int, _c_int, _vp]),
+    "pfsoft_shard_destroy": (None, [_vp]),
+    "pfsoft_shard_layers": (_c_int, [_vp, _c_int, _vp, _vp]),
+    "pfsoft_shard_classes": (_c_int, [_vp, _c_int, _vp, _c_int]),
+    "pfsoft_shard_bins": (ctypes.c_longlong, [_vp, _c_int, _vp, ctypes.c_longlong]),
+    "pfsoft_shard_counts": (_c_int, [_vp, _c_int, _vp, _vp]),
+    "pfsoft_shard_runs": (ctypes.c_longlong, [_vp, _c_int, _c_int, _vp, _vp, _vp, _vp, ctypes.c_longlong]),
+    "pfsoft_shard_fft_forward": (_c_int, [_vp, _vp, _vp, _vp]),
+    "pfsoft_shard_dwt_forward": (_c_int, [_vp, _vp, _vp, _vp]),
+    "pfsoft_shard_dwt_inverse": (_c_int, [_vp, _vp, _vp, _vp]),
+    "pfsoft_shard_fft_inverse": (_c_int, [_vp, _vp, _vp, _vp]),
+    "pfsoft_shard_scatter": (_c_int, [_vp, _c_int, _vp, _vp, _vp]),
+    "pfsoft_shard_pack": (_c_int, [_vp, _c_int, _vp, _vp, _vp]),
+    "pfsoft_shard_unpack": (_c_int, [_vp, _c_int, _vp, _vp, _vp]),
     "pfsoft_profile_enable": (_c_int, [_c_int]),
     "pfsoft_profile_read": (_c_int, [_vp, _vp, _c_int]),
     "pfsoft_profile_stage_name": (ctypes.c_char_p, [_c_int]),

@@ -212,21 +212,7 @@ FftPassArgs pass_args(int n, int nvec, const BandTables& t, FftStrides src, FftS
     return a;
 }
 
-DwtArgs dwt_args(const BandTables& t)
-{
-    DwtArgs a;
-    a.B = t.B;
-    a.N = t.N;
-    a.cosb = t.cosb;
-    a.sinh = t.sinh;
-    a.cosh = t.cosh;
-    a.w = t.w;
-    a.normf = t.normf;
-    a.pw_sin = t.pw_sin;
-    a.pw_cos = t.pw_cos;
-    a.team_warps = dwt_team_warps(t.N);
-    return a;
-}
+DwtArgs dwt_args(const BandTables& t) { return dwt_args_for(t); }
 
 int check_transform_args(const void* a, const void* b, int B, void*& ws, size_t ws_bytes)
 {

@@ -113,17 +113,7 @@ cudaError_t zero_nyquist_launch(double2** ws, int B, int T, cudaStream_t s)
 cudaError_t dwt_per_transform(int dir, const BandTables& t, int T, double2* const* X, double2* const* coeffs,
                               cudaStream_t s)
 {
-    DwtArgs a;
-    a.B = t.B;
-    a.N = t.N;
-    a.cosb = t.cosb;
-    a.sinh = t.sinh;
-    a.cosh = t.cosh;
-    a.w = t.w;
-    a.normf = t.normf;
-    a.pw_sin = t.pw_sin;
-    a.pw_cos = t.pw_cos;
-    a.team_warps = dwt_team_warps(t.N);
+    const DwtArgs a = dwt_args_for(t);
     for (int i = 0; i < T; ++i) {
         cudaError_t e = dir == 0 ? dwt_forward_launch(X[i], coeffs[i], a, 0, s) : dwt_inverse_launch(coeffs[i], X[i], a, 0, s);
         if (e != cudaSuccess) return e;

@@ -105,7 +105,7 @@ __global__ void __launch_bounds__(kWarps * 32, fwd_min_blocks(KT, TW, CS))
     double* s_rc = smem + L::rc_off + (size_t)tm.warp * kLB * 4;
     double* s_red = smem + L::red_off;   // [2][warp][8][16]
     const int B = a.B, N = a.N;
-    const int ncls = num_classes(B);
+    const int ncls = list_length(a);
     const double norm = kPi / (double)(B * 2 * B);   // src/fn_dsoft.cpp:119
 
     int kc[KT];
@@ -120,8 +120,9 @@ __global__ void __launch_bounds__(kWarps * 32, fwd_min_blocks(KT, TW, CS))
     const int my = blockIdx.x * TM::PER_CTA + tm.team;
     int redbuf = 0;
     for (int r = 0;; ++r) {
-        const int cls = snake_class(r, T, my);
-        if (cls >= ncls) break;
+        const int ci = snake_class(r, T, my);
+        if (ci >= ncls) break;
+        const int cls = list_class(a, ci);
         int M, Mp;
         class_orders(cls, M, Mp);
         const int nc = class_case_count(M, Mp);
@@ -152,7 +153,7 @@ __global__ void __launch_bounds__(kWarps * 32, fwd_min_blocks(KT, TW, CS))
             const int nx = snake_class(r + 1, T, my);
             if (nx < ncls && lane < 8) {
                 int M2, Mp2;
-                class_orders(nx, M2, Mp2);
+                class_orders(list_class(a, nx), M2, Mp2);
                 if (lane < class_case_count(M2, Mp2)) {
                     const PairCase p = class_case(M2, Mp2, lane, N);
                     const int k0 = tm.cw * KW, k1 = min(N, k0 + KW);
@@ -281,7 +282,7 @@ __global__ void __launch_bounds__(kWarps * 32, inv_min_blocks(KT, TW, CS))
     constexpr bool kCaseFirst = kWarps / (TW * CS) == 1;
     double* s_g = smem + L::g_off + (size_t)tm.team * 2 * kLB * GS;   // [2][kLB][GS]
     const int B = a.B, N = a.N;
-    const int ncls = num_classes(B);
+    const int ncls = list_length(a);
     const double norm = (double)(B * 2 * B) / kPi;   // src/fn_idsoft.cpp:109
 
     int kc[KT];
@@ -321,17 +322,17 @@ __global__ void __launch_bounds__(kWarps * 32, inv_min_blocks(KT, TW, CS))
 
     const int T = gridDim.x * TM::PER_CTA;
     const int my = blockIdx.x * TM::PER_CTA + tm.team;
-    int cls = snake_class(0, T, my);
+    int ci = snake_class(0, T, my);
     int M = 0, Mp = 0;
-    if (cls < ncls) {
-        class_orders(cls, M, Mp);
+    if (ci < ncls) {
+        class_orders(list_class(a, ci), M, Mp);
         fetch(M, Mp, M);
     }
-    for (int r = 0; cls < ncls; ++r) {
+    for (int r = 0; ci < ncls; ++r) {
         const int nc = class_case_count(M, Mp);
         const int nxt = snake_class(r + 1, T, my);
         int M2 = 0, Mp2 = 0;
-        if (nxt < ncls) class_orders(nxt, M2, Mp2);
+        if (nxt < ncls) class_orders(list_class(a, nxt), M2, Mp2);
 
         double acc[NSUB8][NT][2];
 #pragma unroll
@@ -339,7 +340,7 @@ __global__ void __launch_bounds__(kWarps * 32, inv_min_blocks(KT, TW, CS))
 #pragma unroll
             for (int n = 0; n < NT; ++n) acc[p][n][0] = acc[p][n][1] = 0.0;
 
-        cs.seed(a, kc, a.normf[cls], false, M, Mp);
+        cs.seed(a, kc, a.normf[list_class(a, ci)], false, M, Mp);
         team_sync<TM::WARPS>(tm.team);   // the previous class is done with s_g
         stash(0);                        // chunk 0 (fetched ahead)
         fill_rc4(s_rc, M, M, Mp, lane);
@@ -434,7 +435,7 @@ __global__ void __launch_bounds__(kWarps * 32, inv_min_blocks(KT, TW, CS))
                 }
             }
         }
-        cls = nxt;
+        ci = nxt;
         M = M2;
         Mp = Mp2;
     }
@@ -496,6 +497,24 @@ cudaError_t launch_inv(const double2* coeffs, double2* X, const DwtArgs& a, int 
 }
 
 }  // namespace
+
+DwtArgs dwt_args_for(const BandTables& t)
+{
+    DwtArgs a;
+    a.B = t.B;
+    a.N = t.N;
+    a.cosb = t.cosb;
+    a.sinh = t.sinh;
+    a.cosh = t.cosh;
+    a.w = t.w;
+    a.normf = t.normf;
+    a.pw_sin = t.pw_sin;
+    a.pw_cos = t.pw_cos;
+    a.team_warps = dwt_team_warps(t.N);
+    a.classes = nullptr;
+    a.n_classes = 0;
+    return a;
+}
 
 int dwt_team_warps(int N)
 {

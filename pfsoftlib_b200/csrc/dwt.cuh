@@ -36,7 +36,14 @@ struct DwtArgs {
     const double2* pw_sin;
     const double2* pw_cos;
     int team_warps;   // warps cooperating on one order class (1..4)
+    // Optional subset of order classes (ascending, so longest first): when set, the kernels run
+    // classes[0 .. n_classes-1] only and leave every other class's outputs untouched.
+    const int* classes;
+    int n_classes;
 };
+
+// Arguments of the DWT launches over every order class of a bandwidth's tables.
+DwtArgs dwt_args_for(const BandTables& t);
 
 // nblocks <= 0 launches the persistent grid (all resident CTAs).
 // Forward: X (beta-innermost spectrum, N^3) -> packed coefficients, scale pi/(2B^2).

@@ -83,6 +83,11 @@ __device__ __forceinline__ void prefetch_l2(const void* p, unsigned bytes)
 // classes r*T + my in even rounds and r*T + T-1-my in odd rounds.
 __device__ __forceinline__ int snake_class(int r, int T, int my) { return r * T + ((r & 1) ? (T - 1 - my) : my); }
 
+// Length of the launch's class list and its i-th class (all classes in order when no subset is
+// given; a subset keeps the longest-first order the snake relies on).
+__device__ __forceinline__ int list_length(const DwtArgs& a) { return a.classes ? a.n_classes : num_classes(a.B); }
+__device__ __forceinline__ int list_class(const DwtArgs& a, int i) { return a.classes ? __ldg(a.classes + i) : i; }
+
 template <int KT>
 struct ColumnState {
     double cb[KT], dcur[KT], dprev[KT], keep[KT];

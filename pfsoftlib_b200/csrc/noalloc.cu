@@ -110,17 +110,7 @@ int pfsoft_cuda_dsoft_noalloc(const double* d_grid, int B, double* d_coeffs, voi
     if (fft_pass_launch(reinterpret_cast<const double2*>(d_grid), X, f1, N, -1, s) != cudaSuccess ||
         fft_pass_launch(X, X, f2, N, -1, s) != cudaSuccess)
         return fail(PFSOFT_ECUDA, "pfsoft_cuda_dsoft_noalloc: FFT launch failed");
-    DwtArgs a;
-    a.B = B;
-    a.N = N;
-    a.cosb = t.cosb;
-    a.sinh = t.sinh;
-    a.cosh = t.cosh;
-    a.w = t.w;
-    a.normf = t.normf;
-    a.pw_sin = t.pw_sin;
-    a.pw_cos = t.pw_cos;
-    a.team_warps = dwt_team_warps(N);
+    const DwtArgs a = dwt_args_for(t);
     if (dwt_forward_launch(X, reinterpret_cast<double2*>(d_coeffs), a, 0, s) != cudaSuccess)
         return fail(PFSOFT_ECUDA, "pfsoft_cuda_dsoft_noalloc: DWT launch failed");
     return PFSOFT_OK;
