@@ -200,6 +200,94 @@ __device__ __forceinline__ void run_stage_fixed(const FftPassArgs& a, int s, con
     }
 }
 
+// One stage of a CTA whose every thread owns at most one butterfly (nv * n / R <= blockDim.x),
+// on a single shared buffer: a middle stage reads its inputs, waits for the whole CTA, then
+// overwrites the buffer with its outputs. All threads reach the barrier.
+template <int SIGN, int R>
+__device__ __forceinline__ void run_stage_inplace(const FftPassArgs& a, int s, const double2* gsrc,
+                                                  double2* gdst, double2* buf, int nv,
+                                                  long long src_base, long long dst_base)
+{
+    const int n = a.n;
+    const int m = n / R;
+    const int Ns = a.ns[s];
+    const int step = n / (Ns * R);
+    const bool first = (s == 0), last = (s == a.nstages - 1);
+    const int pl = padded_len(n);
+    const bool kk_fast = (first && a.src.se != 1) || (last && a.dst.se != 1);
+    const int t = threadIdx.x;
+    const bool act = t < nv * m;
+    int j, kk;
+    if (kk_fast) {
+        kk = t % nv;
+        j = t / nv;
+    } else {
+        j = t % m;
+        kk = t / m;
+    }
+    double2 v[R];
+    if (act) {
+        if (first) {
+            const double2* p = gsrc + src_base + (long long)kk * a.src.sv;
+#pragma unroll
+            for (int r = 0; r < R; ++r) v[r] = __ldg(p + (long long)(j + r * m) * a.src.se);
+        } else {
+            const double2* p = buf + kk * pl;
+#pragma unroll
+            for (int r = 0; r < R; ++r) v[r] = p[spos(j + r * m)];
+        }
+    }
+    if (!first && !last) __syncthreads();   // every input read before any output lands
+    if (!act) return;
+    const int k = j % Ns;
+    if (Ns > 1) {
+#pragma unroll
+        for (int r = 1; r < R; ++r) v[r] = cmul(v[r], twiddle(a.twiddle, r * k * step, SIGN));
+    }
+    if (R == 2) dft2<SIGN>(v);
+    else if (R == 4) dft4<SIGN>(v[0], v[1], v[2], v[3]);
+    else if (R == 8) dft8<SIGN>(v);
+    else if (R == 3) dft3<SIGN>(v);
+    else if (R == 5) dft5<SIGN>(v);
+    const int ob = (j / Ns) * Ns * R + k;
+    if (last) {
+        double2* p = gdst + dst_base + (long long)kk * a.dst.sv;
+#pragma unroll
+        for (int q = 0; q < R; ++q) p[(long long)(ob + q * Ns) * a.dst.se] = cscale(v[q], a.scale);
+    } else {
+        double2* p = buf + kk * pl;
+#pragma unroll
+        for (int q = 0; q < R; ++q) p[spos(ob + q * Ns)] = v[q];
+    }
+}
+
+// Passes of three or more radix-8 stages (n = 512): one butterfly per thread per stage and one
+// shared buffer updated in place (35 KB for 4 vectors), so that four CTAs of 8 warps fit on
+// each SM (64 registers a thread) where the ping-pong kernel keeps two. Measured on B200 at
+// n = 512: 1.2-1.26 ms per pass over 2 x 2.1 GB against 1.51-1.56 ms; 8-vector tiles with two
+// 16-warp CTAs per SM came within 2 %.
+template <int SIGN>
+__global__ void __launch_bounds__(256, 4) fft_pass_inplace_kernel(const double2* src, double2* dst,
+                                                                  const FftPassArgs a)
+{
+    extern __shared__ double2 smem[];
+    if (a.srcs) {
+        src = a.srcs[blockIdx.z];
+        dst = a.dsts[blockIdx.z];
+    }
+    const int v0 = blockIdx.x * a.kb;
+    const int nv = min(a.kb, a.nvec - v0);
+    const long long src_base = (long long)v0 * a.src.sv + (long long)blockIdx.y * a.src.sb;
+    const long long dst_base = (long long)v0 * a.dst.sv + (long long)blockIdx.y * a.dst.sb;
+    for (int s = 0; s < a.nstages; ++s) {
+        switch (a.radix[s]) {
+            case 8: run_stage_inplace<SIGN, 8>(a, s, src, dst, smem, nv, src_base, dst_base); break;
+            default: break;
+        }
+        if (s + 1 < a.nstages) __syncthreads();
+    }
+}
+
 // Direct O(R^2) butterfly for any other radix (rare lengths with a large prime factor).
 template <int SIGN>
 __device__ void run_stage_generic(const FftPassArgs& a, int s, const double2* gsrc,
@@ -321,35 +409,71 @@ int fft_plan_radices(int n, int* radix, int* ns)
     return cnt;
 }
 
+namespace {
+
+constexpr int kInplaceThreads = 256;
+
+// Plans of three or more stages, all of radix 8, run the in-place kernel (other radices in the
+// same kernel cost it its 64-register budget).
+bool inplace_plan(int nstages, const int* radix)
+{
+    if (nstages < 3) return false;
+    for (int s = 0; s < nstages; ++s)
+        if (radix[s] != 8) return false;
+    return true;
+}
+
+int widest_stage(int n, int nstages, const int* radix)
+{
+    int w = 1;
+    for (int s = 0; s < nstages; ++s) w = n / radix[s] > w ? n / radix[s] : w;
+    return w;
+}
+
+}  // namespace
+
 int fft_tile_vectors(int n)
 {
+    int radix[kFftMaxStages], ns[kFftMaxStages];
+    const int st = fft_plan_radices(n, radix, ns);
+    if (inplace_plan(st, radix)) {
+        int kb = 8;
+        while (kb > 1 && kb * widest_stage(n, st, radix) > kInplaceThreads) kb >>= 1;
+        return kb;
+    }
     const size_t two_buffers = 2 * (size_t)8 * padded_len(n) * sizeof(double2);
     return two_buffers > (size_t)110 * 1024 ? 4 : 8;
 }
 
 size_t fft_pass_smem_bytes(const FftPassArgs& a)
 {
-    const int buffers = a.nstages >= 3 ? 2 : (a.nstages == 2 ? 1 : 0);
+    const bool ip = inplace_plan(a.nstages, a.radix) && a.kb * widest_stage(a.n, a.nstages, a.radix) <= kInplaceThreads;
+    const int buffers = ip ? 1 : (a.nstages >= 3 ? 2 : (a.nstages == 2 ? 1 : 0));
     return (size_t)buffers * a.kb * padded_len(a.n) * sizeof(double2);
 }
 
 cudaError_t fft_pass_launch(const double2* src, double2* dst, const FftPassArgs& a, int ntiles, int sign,
                             cudaStream_t stream, int nz)
 {
-    // one butterfly per thread in the widest stage, up to 256 threads
-    int widest = 1;
-    for (int s = 0; s < a.nstages; ++s) widest = a.n / a.radix[s] > widest ? a.n / a.radix[s] : widest;
+    // one butterfly per thread in the widest stage, up to 256 threads (the in-place kernel needs
+    // every butterfly of a stage in flight at once: its tiles are sized for that)
+    const int widest = widest_stage(a.n, a.nstages, a.radix);
+    const bool ip = inplace_plan(a.nstages, a.radix) && a.kb * widest <= kInplaceThreads;
     int nthreads = ((a.kb * widest + 31) / 32) * 32;
-    if (nthreads > 256) nthreads = 256;
+    if (!ip && nthreads > 256) nthreads = 256;
     dim3 grid((a.nvec + a.kb - 1) / a.kb, ntiles, nz);
-    size_t smem = fft_pass_smem_bytes(a);
-    // the kernel indexes two buffers; with a single buffer the second pointer is never used
-    if (sign < 0) {
-        if (smem > 48 * 1024) cudaFuncSetAttribute(fft_pass_kernel<-1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        fft_pass_kernel<-1><<<grid, nthreads, smem, stream>>>(src, dst, a);
+    const size_t smem = fft_pass_smem_bytes(a);
+    auto go = [&](auto kern) {
+        if (smem > 48 * 1024) cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        kern<<<grid, nthreads, smem, stream>>>(src, dst, a);
+    };
+    // the ping-pong kernel indexes two buffers; with a single buffer the second is never used
+    if (ip) {
+        if (sign < 0) go(fft_pass_inplace_kernel<-1>);
+        else go(fft_pass_inplace_kernel<1>);
     } else {
-        if (smem > 48 * 1024) cudaFuncSetAttribute(fft_pass_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        fft_pass_kernel<1><<<grid, nthreads, smem, stream>>>(src, dst, a);
+        if (sign < 0) go(fft_pass_kernel<-1>);
+        else go(fft_pass_kernel<1>);
     }
     return cudaGetLastError();
 }

@@ -41,7 +41,9 @@ cudaError_t fft_pass_launch(const double2* src, double2* dst, const FftPassArgs&
 size_t fft_pass_smem_bytes(const FftPassArgs& a);
 
 // Vectors per tile for length n: 8 (128 contiguous bytes on the transposed side) unless the
-// ping-pong buffers of 8 vectors would leave a single CTA per SM (long transforms, n = 512), then 4.
+// ping-pong buffers of 8 vectors would leave a single CTA per SM, then 4; plans of three or more
+// radix-8 stages (n = 512) run the in-place kernel with as many vectors as keep one butterfly
+// per thread (4).
 int fft_tile_vectors(int n);
 
 }  // namespace pfsoft_dev

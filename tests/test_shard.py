@@ -280,7 +280,8 @@ def _emulate(B, P, mode):
 
 @pytest.mark.gpu
 @pytest.mark.parametrize("B,P,mode", [(8, 2, "scatter"), (8, 3, "pack"), (5, 4, "scatter"), (33, 3, "pack"),
-                                      (64, 8, "scatter"), (64, 5, "pack"), (128, 4, "scatter"), (2, 8, "pack")])
+                                      (64, 8, "scatter"), (64, 5, "pack"), (128, 4, "scatter"), (2, 8, "pack"),
+                                      (256, 3, "scatter")])
 def test_emulated_ranks_match_single_gpu(lib, B, P, mode):
     g, coef, back = _emulate(B, P, mode)
     ref = _single(lib, "dsoft", g, B)
