@@ -67,10 +67,11 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="pfsoft", choices=["pfsoft", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", default="single", choices=["single", "mixed", "serve", "b256"],
+    ap.add_argument("--workload", default="single", choices=["single", "mixed", "serve", "b256", "shard"],
                     help="single: the B=128 headline; mixed: 256 transforms of uneven bandwidth, batched "
                          "(FP64 and split precision) and served vs plain loop; serve: Poisson sweep of the server; "
-                         "b256: 64 transforms at B=256 in groups of 8")
+                         "b256: 64 transforms at B=256 in groups of 8; shard: one B=256 transform sharded over "
+                         "the ranks (strong scaling)")
     ap.add_argument("--rates", default="50,100,200,500,1000,2000", help="serve: offered requests/s")
     ap.add_argument("--seconds", type=float, default=2.0, help="serve: arrival window per rate")
     ap.add_argument("--budget-gb", type=float, default=64.0, help="serve: HBM budget of the server's arena")
@@ -440,6 +441,91 @@ def run_b256(args):
     print(json.dumps(line), flush=True)
 
 
+def run_shard(args):
+    """One transform at B = 256 sharded over the N ranks (strong scaling): rank r holds layers
+    [first, first + count) of the 512^3 grid and a balanced share of the order classes; an NCCL
+    all-to-all moves the FFT bins between the stages (pfsoftlib_b200.shard.ShardedTransform).
+    One step = iDSOFT of the coefficients to the ranks' slabs, then DSOFT of the slabs back, the
+    coefficients distributed by order class between the two (each rank holds its classes). The
+    round trip is checked once with the coefficients gathered (all-reduce) before the timing.
+    Timing: barrier + synchronize on both sides of the K steps, max over ranks."""
+    import datetime
+    import socket
+
+    import torch
+    import torch.distributed as dist
+
+    import pfsoftlib_b200
+    from pfsoftlib_b200.shard import ShardedTransform
+
+    rank, world, local = dist_env()
+    torch.cuda.set_device(local)
+    lib = pfsoftlib_b200.load()
+    if "MASTER_ADDR" in os.environ:
+        dist.init_process_group("nccl", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=120))
+    else:
+        with socket.socket() as sk:
+            sk.bind(("127.0.0.1", 0))
+            port = sk.getsockname()[1]
+        dist.init_process_group("nccl", init_method=f"tcp://127.0.0.1:{port}", rank=0, world_size=1,
+                                timeout=datetime.timedelta(seconds=120))
+    B = 256
+    s = torch.cuda.current_stream().cuda_stream
+    coeffs = torch.empty(B * (4 * B * B - 1) // 3, dtype=torch.complex128, device="cuda")
+    assert lib.pfsoft_cuda_random_coeffs(coeffs.data_ptr(), B, 1, 1, 1.0, s) == 0
+    st = ShardedTransform(B)
+    first, count = st.layers
+    slab = torch.empty((count, 2 * B, 2 * B), dtype=torch.complex128, device="cuda")
+    back = torch.empty_like(coeffs)
+
+    part = torch.empty_like(coeffs)
+
+    def step():
+        # coefficients stay distributed by order class between the directions (gather=False)
+        st.idsoft(part, out=slab)
+        st.dsoft(slab, out=part, gather=False)
+
+    st.idsoft(coeffs, out=slab)
+    st.dsoft(slab, out=back)   # gathered once: the round-trip check
+    torch.cuda.synchronize()
+    err = (torch.linalg.vector_norm(back - coeffs) / torch.linalg.vector_norm(coeffs)).item()
+    part.copy_(back)
+    for _ in range(max(args.warmup, 1)):
+        step()
+    steps = max(1, min(args.steps, 20))
+    clocks = ClockSampler(local) if rank == 0 else None
+    if clocks:
+        clocks.start()
+    dist.barrier()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(steps):
+        step()
+    e1.record()
+    torch.cuda.synchronize()
+    dist.barrier()
+    ms = torch.tensor([e0.elapsed_time(e1) / steps], dtype=torch.float64, device="cuda")
+    dist.all_reduce(ms, op=dist.ReduceOp.MAX)
+    clk = clocks.stop() if clocks else None
+    if rank == 0:
+        line = {
+            "metric": "sharded DSOFT+iDSOFT transforms/s of one B=256 transform", "value": 2 / (ms.item() / 1e3),
+            "unit": "transforms/s", "n_gpus": world, "steps": steps, "warmup": max(args.warmup, 1),
+            "ms_per_step": ms.item(), "higher_is_better": True, "scaling": "strong", "vs_baseline": None,
+            "dtype": "f64", "data": "synthetic (device generator, seed 1)",
+            "config": {"workload": "one transform at B=256 sharded over the ranks: layer slabs for the FFT, "
+                                   "order classes for the DWT, NCCL all-to-all between; coefficients "
+                                   "distributed by order class", "B": B, "parallelism": f"shard{world}",
+                       "l2": "inputs far above L2 (512^3 complex128 grid: 2.15 GB)"},
+            "accuracy": {"round_trip_rel_l2": err},
+            "clocks": clk,
+        }
+        print(json.dumps(line), flush=True)
+    del st
+    dist.destroy_process_group()
+
+
 SERVE_BANDS = (16, 24, 32, 48, 64, 96, 128, 192, 256)   # log-spaced: equal weights = log-uniform
 
 
@@ -536,6 +622,9 @@ def main():
         return
     if args.workload == "b256":
         run_b256(args)
+        return
+    if args.workload == "shard":
+        run_shard(args)
         return
 
     import numpy as np

@@ -129,9 +129,17 @@ class ShardPlan:
         _check(coeffs, self.coef_elems(), "coefficients")
         _lib.check(self._lib.pfsoft_shard_dwt_inverse(self._h, _ptr(coeffs), _ptr(spectrum), _stream_handle(stream)))
 
+    def _side(self, direction: int, source: bool) -> tuple[int, str]:
+        """Size and name of the exchange's source (source=True) or destination buffer here."""
+        if direction not in (FORWARD, INVERSE):
+            raise ValueError("direction must be FORWARD or INVERSE")
+        slab = (direction == FORWARD) == source
+        return (self.slab_elems(), "slab spectrum") if slab else (self.spectrum_elems(), "spectrum")
+
     def scatter(self, direction: int, src, dsts, stream=None) -> None:
         """Direct stores into every rank's buffer (dsts: one tensor or device address per rank;
         the spectra in the forward direction, the slab spectra in the inverse)."""
+        _check(src, *self._side(direction, True))
         if len(dsts) != self.nranks:
             raise ValueError(f"expected {self.nranks} destination buffers")
         addr = [0 if d is None else (d if isinstance(d, int) else d.data_ptr()) for d in dsts]
@@ -139,9 +147,13 @@ class ShardPlan:
         _lib.check(self._lib.pfsoft_shard_scatter(self._h, direction, _ptr(src), table, _stream_handle(stream)))
 
     def pack(self, direction: int, src, send, stream=None) -> None:
+        _check(src, *self._side(direction, True))
+        _check(send, sum(self.counts(direction)[0]), "send buffer")
         _lib.check(self._lib.pfsoft_shard_pack(self._h, direction, _ptr(src), _ptr(send), _stream_handle(stream)))
 
     def unpack(self, direction: int, recv, dst, stream=None) -> None:
+        _check(recv, sum(self.counts(direction)[1]), "receive buffer")
+        _check(dst, *self._side(direction, False))
         _lib.check(self._lib.pfsoft_shard_unpack(self._h, direction, _ptr(recv), _ptr(dst), _stream_handle(stream)))
 
     def close(self) -> None:
@@ -208,9 +220,11 @@ class ShardedTransform:
                                group=self.group)
         self.plan.unpack(direction, recv, dst)
 
-    def dsoft(self, slab_grid, out=None):
+    def dsoft(self, slab_grid, out=None, gather: bool = True):
         """DSOFT of the grid whose layers [first, first + count) this rank holds (slab_grid:
-        count * N * N complex values). Returns the whole coefficient vector, on every rank."""
+        count * N * N complex values). Returns the whole coefficient vector on every rank, or with
+        gather=False this rank's part: its classes' coefficients, zero elsewhere (no collective;
+        idsoft accepts it as it is, since each rank reads only its own classes)."""
         import torch.distributed as dist
 
         slab_spec = self._get("slab_spectrum", self.plan.slab_elems())
@@ -219,12 +233,14 @@ class ShardedTransform:
         self.plan.fft_forward(slab_grid.reshape(-1), slab_spec)
         self._exchange(FORWARD, slab_spec, spectrum)
         self.plan.dwt_forward(spectrum, coeffs)
-        dist.all_reduce(_as_real(coeffs), group=self.group)
+        if gather:
+            dist.all_reduce(_as_real(coeffs), group=self.group)
         return coeffs
 
     def idsoft(self, coeffs, out=None):
-        """iDSOFT of the whole coefficient vector (the same on every rank). Returns this rank's
-        layers [first, first + count) of the grid as a (count, N, N) tensor."""
+        """iDSOFT of a coefficient vector: the whole vector, or this rank's part of it (only the
+        rank's own classes are read). Returns this rank's layers [first, first + count) of the
+        grid as a (count, N, N) tensor."""
         nk = self.layers[1]
         slab_spec = self._get("slab_spectrum", self.plan.slab_elems())
         spectrum = self._get("spectrum", self.plan.spectrum_elems())

@@ -169,6 +169,14 @@ def _gloo_rank(rank, world, port, B, errq):
         S2[:, B] = 0
         g2 = np.fft.ifft2(S2.transpose(2, 1, 0), axes=(1, 2))
         assert np.allclose(slab.numpy(), g2[first:first + count], rtol=0, atol=1e-13), "inverse"
+        # coefficients left distributed by class: each rank's part feeds its own inverse
+        part = st.dsoft(torch.from_numpy(grid[first:first + count].copy()), gather=False)
+        own = np.zeros(N * N, bool)
+        own[st.plan.own] = True
+        assert not part.numpy().reshape(N * N, N)[~own].any(), "partial vector outside own bins"
+        slab = st.idsoft(part)
+        g3 = np.fft.ifft2(ref.transpose(2, 1, 0), axes=(1, 2))
+        assert np.allclose(slab.numpy(), g3[first:first + count], rtol=0, atol=1e-12), "distributed round trip"
         dist.barrier()
         dist.destroy_process_group()
     except BaseException as e:   # reported to the parent
