@@ -200,10 +200,11 @@ __device__ __forceinline__ void run_stage_fixed(const FftPassArgs& a, int s, con
     }
 }
 
-// One stage of a CTA whose every thread owns at most one butterfly (nv * n / R <= blockDim.x),
-// on a single shared buffer: a middle stage reads its inputs, waits for the whole CTA, then
-// overwrites the buffer with its outputs. All threads reach the barrier.
-template <int SIGN, int R>
+// One stage of the in-place kernel: each thread owns up to P butterflies of radix R (its
+// threadIdx.x + p * blockDim.x), on a single shared buffer. A stage that reads shared memory and
+// writes it (a middle stage) loads all of its inputs, waits for the whole CTA, then overwrites
+// the buffer with its outputs. All threads reach the barrier.
+template <int SIGN, int R, int P>
 __device__ __forceinline__ void run_stage_inplace(const FftPassArgs& a, int s, const double2* gsrc,
                                                   double2* gdst, double2* buf, int nv,
                                                   long long src_base, long long dst_base)
@@ -215,58 +216,67 @@ __device__ __forceinline__ void run_stage_inplace(const FftPassArgs& a, int s, c
     const bool first = (s == 0), last = (s == a.nstages - 1);
     const int pl = padded_len(n);
     const bool kk_fast = (first && a.src.se != 1) || (last && a.dst.se != 1);
-    const int t = threadIdx.x;
-    const bool act = t < nv * m;
-    int j, kk;
-    if (kk_fast) {
-        kk = t % nv;
-        j = t / nv;
-    } else {
-        j = t % m;
-        kk = t / m;
-    }
-    double2 v[R];
-    if (act) {
-        if (first) {
-            const double2* p = gsrc + src_base + (long long)kk * a.src.sv;
+    int j[P], kk[P];
+    bool act[P];
+    double2 v[P][R];
 #pragma unroll
-            for (int r = 0; r < R; ++r) v[r] = __ldg(p + (long long)(j + r * m) * a.src.se);
+    for (int p = 0; p < P; ++p) {
+        const int t = threadIdx.x + p * blockDim.x;
+        act[p] = t < nv * m;
+        if (kk_fast) {
+            kk[p] = t % nv;
+            j[p] = t / nv;
         } else {
-            const double2* p = buf + kk * pl;
+            j[p] = t % m;
+            kk[p] = t / m;
+        }
+        if (act[p]) {
+            if (first) {
+                const double2* q = gsrc + src_base + (long long)kk[p] * a.src.sv;
 #pragma unroll
-            for (int r = 0; r < R; ++r) v[r] = p[spos(j + r * m)];
+                for (int r = 0; r < R; ++r) v[p][r] = __ldg(q + (long long)(j[p] + r * m) * a.src.se);
+            } else {
+                const double2* q = buf + kk[p] * pl;
+#pragma unroll
+                for (int r = 0; r < R; ++r) v[p][r] = q[spos(j[p] + r * m)];
+            }
         }
     }
     if (!first && !last) __syncthreads();   // every input read before any output lands
-    if (!act) return;
-    const int k = j % Ns;
-    if (Ns > 1) {
 #pragma unroll
-        for (int r = 1; r < R; ++r) v[r] = cmul(v[r], twiddle(a.twiddle, r * k * step, SIGN));
-    }
-    if (R == 2) dft2<SIGN>(v);
-    else if (R == 4) dft4<SIGN>(v[0], v[1], v[2], v[3]);
-    else if (R == 8) dft8<SIGN>(v);
-    else if (R == 3) dft3<SIGN>(v);
-    else if (R == 5) dft5<SIGN>(v);
-    const int ob = (j / Ns) * Ns * R + k;
-    if (last) {
-        double2* p = gdst + dst_base + (long long)kk * a.dst.sv;
+    for (int p = 0; p < P; ++p) {
+        if (!act[p]) continue;
+        const int k = j[p] % Ns;
+        if (Ns > 1) {
 #pragma unroll
-        for (int q = 0; q < R; ++q) p[(long long)(ob + q * Ns) * a.dst.se] = cscale(v[q], a.scale);
-    } else {
-        double2* p = buf + kk * pl;
+            for (int r = 1; r < R; ++r) v[p][r] = cmul(v[p][r], twiddle(a.twiddle, r * k * step, SIGN));
+        }
+        if (R == 2) dft2<SIGN>(v[p]);
+        else if (R == 4) dft4<SIGN>(v[p][0], v[p][1], v[p][2], v[p][3]);
+        else if (R == 8) dft8<SIGN>(v[p]);
+        else if (R == 3) dft3<SIGN>(v[p]);
+        else if (R == 5) dft5<SIGN>(v[p]);
+        const int ob = (j[p] / Ns) * Ns * R + k;
+        if (last) {
+            double2* q = gdst + dst_base + (long long)kk[p] * a.dst.sv;
 #pragma unroll
-        for (int q = 0; q < R; ++q) p[spos(ob + q * Ns)] = v[q];
+            for (int c = 0; c < R; ++c) q[(long long)(ob + c * Ns) * a.dst.se] = cscale(v[p][c], a.scale);
+        } else {
+            double2* q = buf + kk[p] * pl;
+#pragma unroll
+            for (int c = 0; c < R; ++c) q[spos(ob + c * Ns)] = v[p][c];
+        }
     }
 }
 
-// Passes of three or more radix-8 stages (n = 512): one butterfly per thread per stage and one
-// shared buffer updated in place (35 KB for 4 vectors), so that four CTAs of 8 warps fit on
-// each SM (64 registers a thread) where the ping-pong kernel keeps two. Measured on B200 at
-// n = 512: 1.2-1.26 ms per pass over 2 x 2.1 GB against 1.51-1.56 ms; 8-vector tiles with two
-// 16-warp CTAs per SM came within 2 %.
-template <int SIGN>
+// In-place passes for the lengths of kInplacePlans: the radices (R3 = 0: three stages) and the
+// butterflies per thread of each stage are compile-time, so that no stage's registers are
+// reserved for another's radix. One shared buffer (the ping-pong kernel needs two at three or
+// more stages) and 64 registers a thread keep four CTAs of 8 warps on each SM. Measured on
+// B200, per pass against the ping-pong kernel: n = 512 1.2-1.26 ms (1.51-1.56), n = 384 529-560
+// us (623-650), n = 192 50-54 us (84-90), n = 96 12.6 us (18.7-19.0); at n = 512, 8-vector tiles
+// with two 16-warp CTAs per SM came within 2 %.
+template <int SIGN, int R0, int R1, int R2, int R3, int P0, int P1, int P2, int P3>
 __global__ void __launch_bounds__(256, 4) fft_pass_inplace_kernel(const double2* src, double2* dst,
                                                                   const FftPassArgs a)
 {
@@ -279,12 +289,23 @@ __global__ void __launch_bounds__(256, 4) fft_pass_inplace_kernel(const double2*
     const int nv = min(a.kb, a.nvec - v0);
     const long long src_base = (long long)v0 * a.src.sv + (long long)blockIdx.y * a.src.sb;
     const long long dst_base = (long long)v0 * a.dst.sv + (long long)blockIdx.y * a.dst.sb;
-    for (int s = 0; s < a.nstages; ++s) {
-        switch (a.radix[s]) {
-            case 8: run_stage_inplace<SIGN, 8>(a, s, src, dst, smem, nv, src_base, dst_base); break;
-            default: break;
+    if constexpr (R0 == R1 && R1 == R2 && R3 == 0 && P0 == P1 && P1 == P2) {
+        // one radix throughout (n = 512): a loop over the runtime stage count, which compiles
+        // to fewer spills at 64 registers than the unrolled stages
+        for (int s = 0; s < a.nstages; ++s) {
+            run_stage_inplace<SIGN, R0, P0>(a, s, src, dst, smem, nv, src_base, dst_base);
+            if (s + 1 < a.nstages) __syncthreads();
         }
-        if (s + 1 < a.nstages) __syncthreads();
+    } else {
+        run_stage_inplace<SIGN, R0, P0>(a, 0, src, dst, smem, nv, src_base, dst_base);
+        __syncthreads();
+        run_stage_inplace<SIGN, R1, P1>(a, 1, src, dst, smem, nv, src_base, dst_base);
+        __syncthreads();
+        run_stage_inplace<SIGN, R2, P2>(a, 2, src, dst, smem, nv, src_base, dst_base);
+        if constexpr (R3 != 0) {
+            __syncthreads();
+            run_stage_inplace<SIGN, R3, P3>(a, 3, src, dst, smem, nv, src_base, dst_base);
+        }
     }
 }
 
@@ -365,11 +386,51 @@ __global__ void __launch_bounds__(256, 2) fft_pass_kernel(const double2* src, do
     }
 }
 
+// Lengths that run the in-place kernel: tile vectors and radices (0 ends a three-stage plan).
+// 384 is planned 8.4.4.3 rather than 16.8.3: radix 16 does not fit the kernel's 64 registers.
+struct InplacePlan {
+    int n, kb, nstages;
+    int radix[4];
+};
+constexpr InplacePlan kInplacePlans[] = {
+    {512, 4, 3, {8, 8, 8, 0}},
+    {384, 4, 4, {8, 4, 4, 3}},
+    {192, 8, 3, {8, 8, 3, 0}},
+    {96, 8, 3, {8, 4, 3, 0}},
+};
+
+const InplacePlan* inplace_plan_for(int n)
+{
+    for (const InplacePlan& p : kInplacePlans)
+        if (p.n == n) return &p;
+    return nullptr;
+}
+
+// The in-place plan that a pass's arguments follow, if any (the caller may have chosen other
+// tiles or radices; those run the ping-pong kernel).
+const InplacePlan* inplace_plan_of(const FftPassArgs& a)
+{
+    const InplacePlan* p = inplace_plan_for(a.n);
+    if (!p || a.kb != p->kb || a.nstages != p->nstages) return nullptr;
+    for (int s = 0; s < p->nstages; ++s)
+        if (a.radix[s] != p->radix[s]) return nullptr;
+    return p;
+}
+
 }  // namespace
 
 int fft_plan_radices(int n, int* radix, int* ns)
 {
     if (n < 1) return 0;
+    if (const InplacePlan* ip = inplace_plan_for(n)) {
+        int nsv = 1;
+        for (int i = 0; i < ip->nstages; ++i) {
+            radix[i] = ip->radix[i];
+            ns[i] = nsv;
+            nsv *= ip->radix[i];
+        }
+        return ip->nstages;
+    }
     int r[64];
     int cnt = 0, rem = n;
     int p2 = 0;
@@ -409,71 +470,50 @@ int fft_plan_radices(int n, int* radix, int* ns)
     return cnt;
 }
 
-namespace {
-
-constexpr int kInplaceThreads = 256;
-
-// Plans of three or more stages, all of radix 8, run the in-place kernel (other radices in the
-// same kernel cost it its 64-register budget).
-bool inplace_plan(int nstages, const int* radix)
-{
-    if (nstages < 3) return false;
-    for (int s = 0; s < nstages; ++s)
-        if (radix[s] != 8) return false;
-    return true;
-}
-
-int widest_stage(int n, int nstages, const int* radix)
-{
-    int w = 1;
-    for (int s = 0; s < nstages; ++s) w = n / radix[s] > w ? n / radix[s] : w;
-    return w;
-}
-
-}  // namespace
-
 int fft_tile_vectors(int n)
 {
-    int radix[kFftMaxStages], ns[kFftMaxStages];
-    const int st = fft_plan_radices(n, radix, ns);
-    if (inplace_plan(st, radix)) {
-        int kb = 8;
-        while (kb > 1 && kb * widest_stage(n, st, radix) > kInplaceThreads) kb >>= 1;
-        return kb;
-    }
+    if (const InplacePlan* ip = inplace_plan_for(n)) return ip->kb;
     const size_t two_buffers = 2 * (size_t)8 * padded_len(n) * sizeof(double2);
     return two_buffers > (size_t)110 * 1024 ? 4 : 8;
 }
 
 size_t fft_pass_smem_bytes(const FftPassArgs& a)
 {
-    const bool ip = inplace_plan(a.nstages, a.radix) && a.kb * widest_stage(a.n, a.nstages, a.radix) <= kInplaceThreads;
-    const int buffers = ip ? 1 : (a.nstages >= 3 ? 2 : (a.nstages == 2 ? 1 : 0));
+    const int buffers = inplace_plan_of(a) ? 1 : (a.nstages >= 3 ? 2 : (a.nstages == 2 ? 1 : 0));
     return (size_t)buffers * a.kb * padded_len(a.n) * sizeof(double2);
 }
 
 cudaError_t fft_pass_launch(const double2* src, double2* dst, const FftPassArgs& a, int ntiles, int sign,
                             cudaStream_t stream, int nz)
 {
-    // one butterfly per thread in the widest stage, up to 256 threads (the in-place kernel needs
-    // every butterfly of a stage in flight at once: its tiles are sized for that)
-    const int widest = widest_stage(a.n, a.nstages, a.radix);
-    const bool ip = inplace_plan(a.nstages, a.radix) && a.kb * widest <= kInplaceThreads;
+    const InplacePlan* ip = inplace_plan_of(a);
+    // one butterfly per thread in the widest stage, up to 256 threads (the in-place kernels run
+    // 256 threads, each with the butterflies per stage their plan gives)
+    int widest = 1;
+    for (int s = 0; s < a.nstages; ++s) widest = a.n / a.radix[s] > widest ? a.n / a.radix[s] : widest;
     int nthreads = ((a.kb * widest + 31) / 32) * 32;
-    if (!ip && nthreads > 256) nthreads = 256;
+    if (ip || nthreads > 256) nthreads = 256;
     dim3 grid((a.nvec + a.kb - 1) / a.kb, ntiles, nz);
     const size_t smem = fft_pass_smem_bytes(a);
     auto go = [&](auto kern) {
         if (smem > 48 * 1024) cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         kern<<<grid, nthreads, smem, stream>>>(src, dst, a);
     };
-    // the ping-pong kernel indexes two buffers; with a single buffer the second is never used
     if (ip) {
-        if (sign < 0) go(fft_pass_inplace_kernel<-1>);
-        else go(fft_pass_inplace_kernel<1>);
+        // butterflies per thread per stage: ceil(kb * n / R / 256)
+        switch (ip->n) {
+            case 512: sign < 0 ? go(fft_pass_inplace_kernel<-1, 8, 8, 8, 0, 1, 1, 1, 1>)
+                               : go(fft_pass_inplace_kernel<1, 8, 8, 8, 0, 1, 1, 1, 1>); break;
+            case 384: sign < 0 ? go(fft_pass_inplace_kernel<-1, 8, 4, 4, 3, 1, 2, 2, 2>)
+                               : go(fft_pass_inplace_kernel<1, 8, 4, 4, 3, 1, 2, 2, 2>); break;
+            case 192: sign < 0 ? go(fft_pass_inplace_kernel<-1, 8, 8, 3, 0, 1, 1, 2, 1>)
+                               : go(fft_pass_inplace_kernel<1, 8, 8, 3, 0, 1, 1, 2, 1>); break;
+            default: sign < 0 ? go(fft_pass_inplace_kernel<-1, 8, 4, 3, 0, 1, 1, 1, 1>)
+                              : go(fft_pass_inplace_kernel<1, 8, 4, 3, 0, 1, 1, 1, 1>); break;
+        }
     } else {
-        if (sign < 0) go(fft_pass_kernel<-1>);
-        else go(fft_pass_kernel<1>);
+        // the ping-pong kernel indexes two buffers; with a single buffer the second is never used
+        sign < 0 ? go(fft_pass_kernel<-1>) : go(fft_pass_kernel<1>);
     }
     return cudaGetLastError();
 }
