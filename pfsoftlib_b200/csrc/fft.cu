@@ -273,9 +273,9 @@ __device__ __forceinline__ void run_stage_inplace(const FftPassArgs& a, int s, c
 // butterflies per thread of each stage are compile-time, so that no stage's registers are
 // reserved for another's radix. One shared buffer (the ping-pong kernel needs two at three or
 // more stages) and 64 registers a thread keep four CTAs of 8 warps on each SM. Measured on
-// B200, per pass against the ping-pong kernel: n = 512 1.2-1.26 ms (1.51-1.56), n = 384 529-560
-// us (623-650), n = 192 50-54 us (84-90), n = 96 12.6 us (18.7-19.0); at n = 512, 8-vector tiles
-// with two 16-warp CTAs per SM came within 2 %.
+// B200, per pass against the ping-pong kernel: n = 512 1.17-1.23 ms (1.51-1.56), n = 384
+// 529-560 us (623-650), n = 192 50-54 us (84-90), n = 96 12.6 us (18.7-19.0), n = 32 6.6 us
+// (8.1-8.7); at n = 512, 8-vector tiles with two 16-warp CTAs per SM came within 2 %.
 template <int SIGN, int R0, int R1, int R2, int R3, int P0, int P1, int P2, int P3>
 __global__ void __launch_bounds__(256, 4) fft_pass_inplace_kernel(const double2* src, double2* dst,
                                                                   const FftPassArgs a)
@@ -300,8 +300,10 @@ __global__ void __launch_bounds__(256, 4) fft_pass_inplace_kernel(const double2*
         run_stage_inplace<SIGN, R0, P0>(a, 0, src, dst, smem, nv, src_base, dst_base);
         __syncthreads();
         run_stage_inplace<SIGN, R1, P1>(a, 1, src, dst, smem, nv, src_base, dst_base);
-        __syncthreads();
-        run_stage_inplace<SIGN, R2, P2>(a, 2, src, dst, smem, nv, src_base, dst_base);
+        if constexpr (R2 != 0) {
+            __syncthreads();
+            run_stage_inplace<SIGN, R2, P2>(a, 2, src, dst, smem, nv, src_base, dst_base);
+        }
         if constexpr (R3 != 0) {
             __syncthreads();
             run_stage_inplace<SIGN, R3, P3>(a, 3, src, dst, smem, nv, src_base, dst_base);
@@ -386,8 +388,10 @@ __global__ void __launch_bounds__(256, 2) fft_pass_kernel(const double2* src, do
     }
 }
 
-// Lengths that run the in-place kernel: tile vectors and radices (0 ends a three-stage plan).
-// 384 is planned 8.4.4.3 rather than 16.8.3: radix 16 does not fit the kernel's 64 registers.
+// Lengths that run the in-place kernel: tile vectors and radices (0 ends a shorter plan). 384 is
+// planned 8.4.4.3 rather than 16.8.3: radix 16 does not fit the kernel's 64 registers. Measured
+// and left on the ping-pong kernel: 256 as 8.8.4 (125 against 96 us per pass: its 16.16 plan
+// has one exchange and one buffer), 128 as 8.4.4 (23 against 19 us), 64 as 8.8 (equal).
 struct InplacePlan {
     int n, kb, nstages;
     int radix[4];
@@ -397,6 +401,7 @@ constexpr InplacePlan kInplacePlans[] = {
     {384, 4, 4, {8, 4, 4, 3}},
     {192, 8, 3, {8, 8, 3, 0}},
     {96, 8, 3, {8, 4, 3, 0}},
+    {32, 8, 2, {8, 4, 0, 0}},
 };
 
 const InplacePlan* inplace_plan_for(int n)
@@ -508,8 +513,11 @@ cudaError_t fft_pass_launch(const double2* src, double2* dst, const FftPassArgs&
                                : go(fft_pass_inplace_kernel<1, 8, 4, 4, 3, 1, 2, 2, 2>); break;
             case 192: sign < 0 ? go(fft_pass_inplace_kernel<-1, 8, 8, 3, 0, 1, 1, 2, 1>)
                                : go(fft_pass_inplace_kernel<1, 8, 8, 3, 0, 1, 1, 2, 1>); break;
-            default: sign < 0 ? go(fft_pass_inplace_kernel<-1, 8, 4, 3, 0, 1, 1, 1, 1>)
+            case 32: sign < 0 ? go(fft_pass_inplace_kernel<-1, 8, 4, 0, 0, 1, 1, 1, 1>)
+                              : go(fft_pass_inplace_kernel<1, 8, 4, 0, 0, 1, 1, 1, 1>); break;
+            case 96: sign < 0 ? go(fft_pass_inplace_kernel<-1, 8, 4, 3, 0, 1, 1, 1, 1>)
                               : go(fft_pass_inplace_kernel<1, 8, 4, 3, 0, 1, 1, 1, 1>); break;
+            default: return cudaErrorInvalidValue;   // a table entry without a kernel
         }
     } else {
         // the ping-pong kernel indexes two buffers; with a single buffer the second is never used
