@@ -227,8 +227,9 @@ int pfsoft_server_reset_stats(pfsoft_server* srv);
  *            any rank's next step: the caller synchronises the ranks in between.
  *   pack, all-to-all, unpack: pack into this rank's send buffer, move it with the caller's
  *            all-to-all (NCCL), unpack from the receive buffer.
- * Device tables are made on the first call that takes a stream, on the current device; a plan
- * serves one device. pfsoft_shard_classes / _bins / _counts / _runs are host-only queries (the
+ * Device tables are made on the first call of each step that takes a stream (allocations and
+ * synchronous copies: make those first calls before any stream capture), on the current
+ * device; a plan serves one device. pfsoft_shard_classes / _bins / _counts / _runs are host-only queries (the
  * classes and bins of a rank, the values sent to and received from each peer, and the copy runs
  * of an exchange step: step 0 scatter, 1 pack, 2 unpack; a run copies len values from
  * src + src_off to buffer `slot` + dst_off). */
