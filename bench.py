@@ -73,8 +73,9 @@ def parse():
                          "b256: 64 transforms at B=256 in groups of 8; shard: one B=256 transform sharded over "
                          "the ranks (strong scaling)")
     ap.add_argument("--rates", default="50,100,200,500,1000,2000", help="serve: offered requests/s")
-    ap.add_argument("--seconds", type=float, default=2.0, help="serve: arrival window per rate")
-    ap.add_argument("--budget-gb", type=float, default=64.0, help="serve: HBM budget of the server's arena")
+    ap.add_argument("--seconds", type=float, default=5.2,
+                    help="serve: arrival window per rate (5.2 s over the default rates: ~20,000 requests)")
+    ap.add_argument("--budget-gb", type=float, default=160.0, help="serve: HBM budget of the server's arena")
     return ap.parse_args()
 
 
@@ -378,7 +379,9 @@ def run_b256(args):
     """64 transforms at B = 256 (|f| = (1+l)^-2 with uniform phase, device generator, seed 3 + i),
     streamed through one batch plan in groups of 8: per group the coefficients are generated, then
     IDSOFT (8 grids of 2.15 GB) and DSOFT of those grids. One step = all 64 IDSOFT + DSOFT; the
-    generation is outside the timed region. Accuracy: round trip of every transform."""
+    generation is outside the timed region. Accuracy: round trip of every transform, and the first
+    grid of the last group against the compiled reference's CPU DSOFT (all host threads) when it is
+    built."""
     import ctypes
 
     import torch
@@ -425,6 +428,19 @@ def run_b256(args):
     clk = clocks.stop()
     lib.pfsoft_batch_destroy(plan)
     ms /= steps
+    acc = {"round_trip_rel_l2_max": worst[0]}
+    # checker: the compiled reference's CPU DSOFT of the last group's first grid, all host threads
+    from oracle import oracle as orc
+    if orc.Reference.available():
+        ref = orc.Reference()
+        g_h = grids[0].cpu().numpy()
+        t0 = time.perf_counter()
+        f_ref = ref.dsoft(g_h, ref.max_threads())
+        acc["vs_reference_dsoft_rel_l2"] = orc.rel_l2(back[0].cpu().numpy(), f_ref)
+        acc["vs_reference_dsoft_max_abs"] = orc.max_abs(back[0].cpu().numpy(), f_ref)
+        acc["reference_dsoft_s"] = time.perf_counter() - t0
+        acc["reference_threads"] = ref.max_threads()
+        del g_h, f_ref
     line = {
         "metric": "DSOFT+iDSOFT transforms/s, 64 transforms at B=256", "value": 2 * T / (ms / 1e3),
         "unit": "transforms/s", "n_gpus": 1, "steps": steps, "warmup": 1, "ms_per_step": ms,
@@ -433,7 +449,7 @@ def run_b256(args):
         "config": {"workload": "64 transforms at B=256 (seed 3+i, |f|=(1+l)^-2), groups of 8 through one "
                                "batch plan; one step = IDSOFT + DSOFT of all 64",
                    "grid": "512^3 complex128 (2.15 GB) each", "l2": "far above L2"},
-        "accuracy": {"round_trip_rel_l2_max": worst[0]},
+        "accuracy": acc,
         "split_precision": "not run: the split-precision DWT covers B = 16..128 (K <= 256 keeps its "
                            "leading digit-plane sums exact in FP32)",
         "clocks": clk,
@@ -558,7 +574,10 @@ def run_serve_sweep(args):
     rng = np.random.default_rng(4)
     rates = [float(r) for r in args.rates.split(",") if r]
     sweep = []
-    budget = int(args.budget_gb * (1 << 30))
+    # the arena is one allocation of the whole budget: cap it by what the device has left after
+    # the request buffers above (4 GiB kept back for tables, staging and the CUDA context)
+    free, _ = torch.cuda.mem_get_info()
+    budget = min(int(args.budget_gb * (1 << 30)), free - (4 << 30))
     with TransformServer(budget_bytes=budget, max_batch=16, streams=4) as srv:
         # warm-up: tables and item lists of every bandwidth and direction
         warm = [srv.submit(d, B, ins[B][d], outs[B][d][0]) for B in SERVE_BANDS for d in (0, 1)]
