@@ -71,7 +71,7 @@ int pfsoft_cuda_idsoft(const double* d_coeffs, int B, double* d_grid, void* d_wo
  * callers that cannot allocate device memory (a framework-owned, capped memory pool; a hard
  * per-process memory limit; a loop that must not take cudaMalloc's locks or cudaFree's device
  * synchronisation): it makes no allocation at all and uses a scratch array that the library
- * holds in device memory from load to exit (4.25 MiB per GPU). Limit: bandwidth B <= 32; a
+ * holds in device memory from load to exit (4.31 MiB per GPU). Limit: bandwidth B <= 32; a
  * larger B returns PFSOFT_EINVAL. The first call on a device looks up that array's device
  * address and builds the tables for B in it; make that first call before any stream capture.
  * All calls on a device share the array, so calls that overlap on the GPU race; nothing in it

@@ -165,7 +165,7 @@ __global__ void __launch_bounds__(kWarps * 32, fwd_min_blocks(KT, TW, CS))
             }
         }
         cs.seed(a, kc, a.normf[cls], true, M, Mp);
-        fill_rc4(s_rc, M, M, Mp, lane);
+        fill_rc4(a, s_rc, M, M, Mp, lane);
 #pragma unroll
         for (int s = 0; s < 8; ++s) gen_step<KT>(cs, s_d + s * DS, lane, s_rc + 4 * s);   // block 0
         __syncwarp();
@@ -193,7 +193,7 @@ __global__ void __launch_bounds__(kWarps * 32, fwd_min_blocks(KT, TW, CS))
                 // contract block blk while generating block blk+1 (degrees beyond B - 1 are
                 // generated too; their rows only reach outputs that are never stored)
                 const int off = 8 * (blk + 1);
-                if ((off & (kLB - 1)) == 0) fill_rc4(s_rc, M + off, M, Mp, lane);
+                if ((off & (kLB - 1)) == 0) fill_rc4(a, s_rc, M + off, M, Mp, lane);
                 const double* rcb = s_rc + 4 * (off & (kLB - 1));
 #pragma unroll
                 for (int s = 0; s < 8; ++s) {
@@ -343,7 +343,7 @@ __global__ void __launch_bounds__(kWarps * 32, inv_min_blocks(KT, TW, CS))
         cs.seed(a, kc, a.normf[list_class(a, ci)], false, M, Mp);
         team_sync<TM::WARPS>(tm.team);   // the previous class is done with s_g
         stash(0);                        // chunk 0 (fetched ahead)
-        fill_rc4(s_rc, M, M, Mp, lane);
+        fill_rc4(a, s_rc, M, M, Mp, lane);
 #pragma unroll
         for (int s = 0; s < 8; ++s) gen_step<KT>(cs, s_d + s * DS, lane, s_rc + 4 * s);   // block 0
         team_sync<TM::WARPS>(tm.team);   // chunk 0 and block 0 rows visible
@@ -401,7 +401,7 @@ __global__ void __launch_bounds__(kWarps * 32, inv_min_blocks(KT, TW, CS))
                 if (boundary) {
                     // publish the prefetched chunk (its buffer was last read two chunks ago)
                     stash((offn >> 5) & 1);
-                    fill_rc4(s_rc, M + offn, M, Mp, lane);
+                    fill_rc4(a, s_rc, M + offn, M, Mp, lane);
                 }
                 const double* rcb = s_rc + 4 * (offn & (kLB - 1));
 #pragma unroll
@@ -511,6 +511,8 @@ DwtArgs dwt_args_for(const BandTables& t)
     a.pw_sin = t.pw_sin;
     a.pw_cos = t.pw_cos;
     a.team_warps = dwt_team_warps(t.N);
+    a.rc_cf = t.rc_cf;
+    a.rc_f1 = t.rc_f1;
     a.classes = nullptr;
     a.n_classes = 0;
     return a;

@@ -19,8 +19,21 @@ struct BandTables {
     double2* twiddle = nullptr; // exp(-2 pi i t / N)             [N]
     double2* pw_sin = nullptr;  // sin(beta_k/2)^p as {mantissa, exponent}  [2B][N], p < 2B
     double2* pw_cos = nullptr;  // cos(beta_k/2)^p as {mantissa, exponent}  [2B][N]
+    // recurrence coefficients of the step l -> l+1 for every order class and degree M <= l < B,
+    // class (M, M') from rc_offset(B, M, M'): {c1, f1 f2} and f1      [rc_entries(B)]
+    double2* rc_cf = nullptr;
+    double* rc_f1 = nullptr;
     void* block = nullptr;      // single allocation holding all of the above
 };
+
+// Entries of the recurrence-coefficient table before class (M, M'): classes run M = 0, 1, ...
+// and M' = 0..M within M, each with B - M degrees.
+__host__ __device__ __forceinline__ long long rc_offset(int B, int M, int Mp)
+{
+    const long long m = M;
+    return (long long)(B + 1) * m * (m + 1) / 2 - m * (m + 1) * (2 * m + 1) / 6 + (long long)Mp * (B - M);
+}
+__host__ __device__ __forceinline__ long long rc_entries(int B) { return rc_offset(B, B, 0); }
 
 size_t tables_bytes(int B);
 // Carve the tables out of `mem` (tables_bytes(B) bytes, 256-byte aligned) and fill them.
@@ -36,6 +49,8 @@ struct DwtArgs {
     const double2* pw_sin;
     const double2* pw_cos;
     int team_warps;   // warps cooperating on one order class (1..4)
+    const double2* rc_cf;   // recurrence coefficients (BandTables::rc_cf / rc_f1)
+    const double* rc_f1;
     // Optional subset of order classes (ascending, so longest first): when set, the kernels run
     // classes[0 .. n_classes-1] only and leave every other class's outputs untouched.
     const int* classes;

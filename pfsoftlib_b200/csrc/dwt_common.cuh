@@ -150,14 +150,20 @@ struct ColumnState {
 };
 
 // Recurrence coefficients for degrees l .. l+31 of one warp: rc[i] = {c1, f1 f2, f1, -} for the
-// step l+i -> l+i+1 (one lane per degree). Steps past the last degree are filled as well (their
-// values stay finite and only feed rows that are never used), so the step loop has no guards.
-__device__ __forceinline__ void fill_rc4(double* rc, int l, int M, int Mp, int lane)
+// step l+i -> l+i+1 (one lane per degree), read from the bandwidth's table. Steps past the last
+// degree get zeros (the rows they feed are zero and never used), so the step loop has no guards.
+__device__ __forceinline__ void fill_rc4(const DwtArgs& a, double* rc, int l, int M, int Mp, int lane)
 {
     __syncwarp();
-    double c1, f1, f2;
-    rec_coef(l + lane, M, Mp, c1, f1, f2);
-    *reinterpret_cast<double2*>(rc + 4 * lane) = make_double2(c1, f1 * f2);
+    const int d = l + lane;
+    double2 cf = make_double2(0.0, 0.0);
+    double f1 = 0.0;
+    if (d < a.B) {
+        const long long i = rc_offset(a.B, M, Mp) + (d - M);
+        cf = __ldg(a.rc_cf + i);
+        f1 = __ldg(a.rc_f1 + i);
+    }
+    *reinterpret_cast<double2*>(rc + 4 * lane) = cf;
     rc[4 * lane + 2] = f1;
     __syncwarp();
 }

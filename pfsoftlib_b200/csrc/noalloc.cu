@@ -31,7 +31,7 @@ namespace {
 
 constexpr int kNoAllocMaxB = 32;
 constexpr size_t kSpectrumBytes = (size_t)(2 * kNoAllocMaxB) * (2 * kNoAllocMaxB) * (2 * kNoAllocMaxB) * sizeof(double2);
-constexpr size_t kTableBytes = 256 * 1024;
+constexpr size_t kTableBytes = 320 * 1024;
 constexpr int kMaxDevices = 64;
 
 // The scratch: spectrum first, tables after it. In host code this name is only a handle for

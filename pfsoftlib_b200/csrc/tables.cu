@@ -4,6 +4,8 @@
 //   w_B(j) = 2/B sin(pi(2j+1)/(4B)) sum_{k<B} sin((2j+1)(2k+1)pi/(4B))/(2k+1)   fn_dwt.hpp:62-83
 //   normf(M,M') = sqrt((2M+1)/2) prod_{i<M-M'} sqrt((2M-i)/(i+1))              fn_dwt.hpp:117-121
 //   twiddle[t] = exp(-2 pi i t/N)
+//   rc_cf / rc_f1: the recurrence coefficients c1, f1 f2 and f1 of every class and degree
+//       (fn_dwt.hpp:167-199), so that the DWT kernels load them instead of recomputing them
 //   pw_sin[p][k], pw_cos[p][k] = sin(beta_k/2)^p, cos(beta_k/2)^p, p < 2B, as an exact binary
 //       exponent and a mantissa in [0.5, 1) (exponentiation by squaring, renormalised each
 //       product), so that Wigner seeds far below the FP64 range keep full relative precision
@@ -12,6 +14,7 @@
 
 #include "common.cuh"
 #include "dwt.cuh"
+#include "dwt_common.cuh"
 
 namespace pfsoft_dev {
 
@@ -98,13 +101,28 @@ __global__ void tables_kernel(int B, double* cosb, double* sinh, double* cosh, d
     }
 }
 
+// One CTA per order class: c1, f1 f2, f1 of the steps l -> l+1, l = M .. B-1.
+__global__ void rc_kernel(int B, double2* rc_cf, double* rc_f1)
+{
+    int M, Mp;
+    class_orders(blockIdx.x, M, Mp);
+    const long long base = rc_offset(B, M, Mp);
+    for (int l = M + threadIdx.x; l < B; l += blockDim.x) {
+        double c1, f1, f2;
+        dwtk::rec_coef(l, M, Mp, c1, f1, f2);
+        rc_cf[base + (l - M)] = make_double2(c1, f1 * f2);
+        rc_f1[base + (l - M)] = f1;
+    }
+}
+
 }  // namespace
 
 size_t tables_bytes(int B)
 {
-    const size_t N = 2 * (size_t)B;
+    const size_t N = 2 * (size_t)B, R = (size_t)rc_entries(B);
     return 4 * align256(N * sizeof(double)) + align256(num_classes(B) * sizeof(double)) +
-           align256(N * sizeof(double2)) + 2 * align256(2 * (size_t)B * N * sizeof(double2));
+           align256(N * sizeof(double2)) + 2 * align256(2 * (size_t)B * N * sizeof(double2)) +
+           align256(R * sizeof(double2)) + align256(R * sizeof(double));
 }
 
 cudaError_t tables_build(int B, void* mem, BandTables* t, cudaStream_t stream)
@@ -129,6 +147,10 @@ cudaError_t tables_build(int B, void* mem, BandTables* t, cudaStream_t stream)
     t->pw_sin = reinterpret_cast<double2*>(p);
     p += align256(2 * (size_t)B * N * sizeof(double2));
     t->pw_cos = reinterpret_cast<double2*>(p);
+    p += align256(2 * (size_t)B * N * sizeof(double2));
+    t->rc_cf = reinterpret_cast<double2*>(p);
+    p += align256((size_t)rc_entries(B) * sizeof(double2));
+    t->rc_f1 = reinterpret_cast<double*>(p);
     const int threads = 128;
     int blocks = (int)((num_classes(B) + threads - 1) / threads);
     if (blocks < 1) blocks = 1;
@@ -139,6 +161,9 @@ cudaError_t tables_build(int B, void* mem, BandTables* t, cudaStream_t stream)
     int pblocks = (int)((total + 255) / 256);
     if (pblocks > 4096) pblocks = 4096;
     powers_kernel<<<pblocks, 256, 0, stream>>>(B, t->sinh, t->cosh, t->pw_sin, t->pw_cos);
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    rc_kernel<<<num_classes(B), 128, 0, stream>>>(B, t->rc_cf, t->rc_f1);
     return cudaGetLastError();
 }
 
