@@ -423,6 +423,8 @@ int pfsoft_batch_create(const int* bandwidths, int count, int transforms_per_cta
         d.normf = g.tables.normf;
         d.pw_sin = g.tables.pw_sin;
         d.pw_cos = g.tables.pw_cos;
+        d.rc_cf = g.tables.rc_cf;
+        d.rc_f1 = g.tables.rc_f1;
         d.X = b->ws_ptrs() + g.ptr_base;
         d.coeffs = b->coef_ptrs() + g.ptr_base;
         dg_f.push_back(d);

@@ -85,6 +85,8 @@ struct DwtGroup {
     const double* normf;
     const double2* pw_sin;
     const double2* pw_cos;
+    const double2* rc_cf;   // recurrence coefficients (BandTables::rc_cf / rc_f1)
+    const double* rc_f1;
     double2* const* X;
     double2* const* coeffs;
 };

@@ -99,12 +99,19 @@ struct GenState {
     }
 };
 
-// Recurrence coefficients for degrees l .. l+31 into rc (warp 0 only; one lane per degree).
-__device__ __forceinline__ void rc_chunk(double* rc, int l, int M, int Mp, int lane)
+// Recurrence coefficients for degrees l .. l+31 into rc (warp 0 only; one lane per degree), from
+// the bandwidth's table; steps past the last degree get zeros (their rows are never used).
+__device__ __forceinline__ void rc_chunk(const DwtGroup& gr, double* rc, int l, int M, int Mp, int lane)
 {
-    double c1, f1, f2;
-    rec_coef(l + lane, M, Mp, c1, f1, f2);
-    *reinterpret_cast<double2*>(rc + 4 * lane) = make_double2(c1, f1 * f2);
+    const int d = l + lane;
+    double2 cf = make_double2(0.0, 0.0);
+    double f1 = 0.0;
+    if (d < gr.B) {
+        const long long i = rc_offset(gr.B, M, Mp) + (d - M);
+        cf = __ldg(gr.rc_cf + i);
+        f1 = __ldg(gr.rc_f1 + i);
+    }
+    *reinterpret_cast<double2*>(rc + 4 * lane) = cf;
     rc[4 * lane + 2] = f1;
 }
 
@@ -170,7 +177,7 @@ __global__ void __launch_bounds__(64 * TT) dwt_batch_kernel(const DwtGroup* __re
                 po = class_case(M, Mp, co < nc ? co : 0, N);
             }
             for (int c0 = M; c0 < B; c0 += kChunk) {
-                if (warp == 0) rc_chunk(s_rc, c0, M, Mp, lane);
+                if (warp == 0) rc_chunk(gr, s_rc, c0, M, Mp, lane);
                 __syncthreads();
 #pragma unroll 4
                 for (int s = 0; s < kChunk; ++s) gs.step(s_d + s * DS, kc, s_rc + 4 * s);
@@ -225,7 +232,7 @@ __global__ void __launch_bounds__(64 * TT) dwt_batch_kernel(const DwtGroup* __re
                     const int t = e / (8 * kChunk), j = (e >> 3) % kChunk, c = e & 7;
                     if (t < TT) *reinterpret_cast<double2*>(s_g + ((size_t)t * kChunk + j) * L::GS + 2 * c) = pf[i];
                 }
-                if (warp == 0) rc_chunk(s_rc, c0, M, Mp, lane);
+                if (warp == 0) rc_chunk(gr, s_rc, c0, M, Mp, lane);
                 __syncthreads();
                 if (c0 + kChunk < B) fetch(c0 + kChunk);   // in flight during this chunk
 #pragma unroll 4

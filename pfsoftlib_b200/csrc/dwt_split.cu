@@ -294,12 +294,12 @@ __global__ void __launch_bounds__(kThreads, 1) dwt_split_kernel(const DwtGroup* 
             wmax = block_max(w, s_red, tid);
             wgroup = it.group;
         }
-        for (int r = tid; r < R; r += kThreads) {
-            double c1, f1, f2;
-            rec_coef(M + r, M, Mp, c1, f1, f2);
-            s_rc[4 * r] = c1;
-            s_rc[4 * r + 1] = f1 * f2;
-            s_rc[4 * r + 2] = f1;
+        const long long rc0 = rc_offset(B, M, Mp);
+        for (int r = tid; r < R; r += kThreads) {   // M + r < B: every row has a table entry
+            const double2 cf = __ldg(gr.rc_cf + rc0 + r);
+            s_rc[4 * r] = cf.x;
+            s_rc[4 * r + 1] = cf.y;
+            s_rc[4 * r + 2] = __ldg(gr.rc_f1 + rc0 + r);
             const double bound = (DIR == 0 ? wmax : 1.0) * sqrt((double)(M + r) + 0.5);
             const double rs = 0.49 / bound;
             s_rs[r] = rs * kTwo47;

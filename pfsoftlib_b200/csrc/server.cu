@@ -201,6 +201,8 @@ int launch_batch(pfsoft_server* s, Batch* b, const std::vector<Request>& io)
     g.normf = t.normf;
     g.pw_sin = t.pw_sin;
     g.pw_cos = t.pw_cos;
+    g.rc_cf = t.rc_cf;
+    g.rc_f1 = t.rc_f1;
     g.X = d_tab + 2 * cap;
     g.coeffs = d_tab + cap;
     std::memcpy(sl.h_stage, &g, sizeof(g));
