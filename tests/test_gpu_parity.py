@@ -86,7 +86,7 @@ def test_idsoft_matches_oracle(lib, oracle, B):
     assert orc.max_abs(grid, ref) <= ABS_TOL * max(1, B)
 
 
-@pytest.mark.parametrize("B", [32, 64, 128])
+@pytest.mark.parametrize("B", [16, 32, 64, 96, 128, 192])
 def test_round_trip_reference_criterion(lib, B):
     c = orc.coeffs_uniform(B, seed=B)
     grid = gpu_idsoft(lib, c, B)
@@ -133,7 +133,8 @@ def test_host_staged_matches_device(lib):
 
 
 @pytest.mark.parametrize("cols,rows,lays", [(8, 8, 3), (32, 32, 5), (24, 40, 2), (7, 9, 3), (256, 256, 2), (512, 512, 1),
-                                             (512, 384, 5), (384, 512, 6)])
+                                             (512, 384, 5), (384, 512, 6), (96, 192, 3), (192, 96, 2),
+                                             (32, 96, 4)])
 def test_layer_wise_fft_matches_numpy(lib, cols, rows, lays):
     rng = np.random.default_rng(cols * rows)
     x = rng.standard_normal((lays, cols, rows)) + 1j * rng.standard_normal((lays, cols, rows))
