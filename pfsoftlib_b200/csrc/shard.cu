@@ -165,11 +165,16 @@ struct pfsoft_shard_plan {
         return PFSOFT_OK;
     }
 
+    // frees the device tables on the device they were made on, then restores the caller's device
     ~pfsoft_shard_plan()
     {
+        if (device < 0) return;
+        int cur = -1;
+        const bool switched = cudaGetDevice(&cur) == cudaSuccess && cur != device && cudaSetDevice(device) == cudaSuccess;
         for (Run* r : d_runs)
             if (r) cudaFree(r);
         if (d_classes) cudaFree(d_classes);
+        if (switched) cudaSetDevice(cur);
     }
 };
 
@@ -184,7 +189,12 @@ int run_copy(pfsoft_shard_plan* plan, int kind, const double* src, const DstTabl
 {
     const Run* d = nullptr;
     long long n = 0;
-    int rc = plan->device_runs(kind, &d, &n);
+    int rc;
+    try {
+        rc = plan->device_runs(kind, &d, &n);
+    } catch (const std::bad_alloc&) {
+        return fail(PFSOFT_ENOMEM, "shard plan: run list allocation");
+    }
     if (rc) return rc;
     if (n == 0) return PFSOFT_OK;
     if (!src) return fail(PFSOFT_EINVAL, "null exchange source buffer");
@@ -220,7 +230,12 @@ int pfsoft_shard_create(int B, int nranks, int rank, pfsoft_shard_plan** out)
     if (rank < 0 || rank >= nranks) return fail(PFSOFT_EINVAL, "rank must be in [0, nranks)");
     pfsoft_shard_plan* p = new (std::nothrow) pfsoft_shard_plan;
     if (!p) return fail(PFSOFT_ENOMEM, "shard plan allocation");
-    p->p = pfsoft_shard::make_plan(B, nranks, rank);
+    try {
+        p->p = pfsoft_shard::make_plan(B, nranks, rank);
+    } catch (const std::bad_alloc&) {
+        delete p;
+        return fail(PFSOFT_ENOMEM, "shard plan allocation");
+    }
     *out = p;
     return PFSOFT_OK;
 }
@@ -272,7 +287,13 @@ long long pfsoft_shard_runs(pfsoft_shard_plan* plan, int direction, int step, lo
     if (!plan || (direction != PFSOFT_SHARD_FORWARD && direction != PFSOFT_SHARD_INVERSE) || step < 0 || step > 2)
         return -1;
     std::lock_guard<std::mutex> lk(plan->mu);
-    const std::vector<Run>& h = plan->host_runs(kind_of(direction, step));
+    const std::vector<Run>* hp = nullptr;
+    try {
+        hp = &plan->host_runs(kind_of(direction, step));
+    } catch (const std::bad_alloc&) {
+        return -1;
+    }
+    const std::vector<Run>& h = *hp;
     for (long long i = 0; i < (long long)h.size() && i < capacity; ++i) {
         if (src_off) src_off[i] = h[i].src_off;
         if (dst_off) dst_off[i] = h[i].dst_off;
