@@ -16,9 +16,10 @@
  *           2l+1+M -- the storage of DSOFTFourierCoefficients
  *           (src/dsoft_fourier_coefficients.cpp:48-57, :80-89), packed contiguously.
  *
- * First use of a bandwidth on a device builds its constant tables (one cudaMalloc and one
- * small kernel, then a stream synchronisation); make that first call before any stream
- * capture. Later calls for the same bandwidth allocate nothing.
+ * First use of a bandwidth on a device builds its constant tables (one cudaMalloc and a few
+ * small kernels, then a stream synchronisation); make that first call before any stream
+ * capture. Later calls for the same bandwidth allocate nothing. The tables stay until exit:
+ * about 11 MB at B = 128, 77 MB at B = 256, 575 MB at B = 512 per bandwidth and device.
  */
 #ifndef PFSOFT_B200_H
 #define PFSOFT_B200_H
