@@ -84,18 +84,19 @@ int pfsoft_cuda_dsoft_noalloc(const double* d_grid, int B, double* d_coeffs, voi
  * transforms by bandwidth; each execution runs batched FFT passes per bandwidth and ONE
  * persistent DWT launch over every (bandwidth, order class, transform block) item, longest
  * first, in which one on-chip Wigner recurrence serves up to `transforms_per_cta` transforms
- * (0 = default: 4 for B <= 64, 2 above). Bandwidths up to 128 share the fused launch; larger
- * ones use the per-transform DWT. The sequence is captured once into a CUDA graph and replayed
+ * (0 = default: 4 for B <= 64, 2 above). Bandwidths up to 128 share the fused FP64 launch;
+ * larger ones use the per-transform FP64 DWT (or the split launch, below). The sequence is captured once into a CUDA graph and replayed
  * (PFSOFT_BATCH_NO_GRAPH disables the graph). The plan owns one spectrum workspace per
  * transform (pfsoft_batch_workspace_bytes). Pointer tables are host arrays of `count` device
  * pointers in the caller's order; every buffer has the single-transform layouts above. Stream
  * ordered. Calls on one plan are serialised by the plan.
- * PFSOFT_BATCH_SPLIT runs the DWT of the bandwidths that pfsoft_split_supported() accepts on the
- * tensor cores instead: the FP64 Wigner rows and FP64 data are cut into six 8-bit digit planes
- * held exactly in bf16, multiplied with FP32 accumulation (exact for the leading planes) and
- * summed in FP64; relative L2 error about 1e-13 against the FP64 path. Four transforms of one
- * bandwidth share each generated Wigner tile. pfsoft_batch_status reports PFSOFT_ETIMEOUT if a
- * bounded wait inside that kernel ever ran out (it synchronises the device). */
+ * PFSOFT_BATCH_SPLIT runs the DWT of the bandwidths that pfsoft_split_supported() accepts
+ * (1 <= B <= 256) on the tensor cores instead, all of them in one launch per direction: the FP64
+ * Wigner rows and FP64 data are cut into six signed 8-bit digit planes, multiplied exactly
+ * (8-bit x 8-bit products summed in 32-bit integers) and combined in FP64; relative L2 error
+ * about 1e-13 against the FP64 path. Two transforms of one bandwidth share each generated Wigner
+ * tile. pfsoft_batch_status reports PFSOFT_ETIMEOUT if a bounded wait inside that kernel ever ran
+ * out (it synchronises the device). */
 #define PFSOFT_BATCH_NO_GRAPH 1
 #define PFSOFT_BATCH_SPLIT 2
 typedef struct pfsoft_batch pfsoft_batch;
@@ -188,6 +189,14 @@ typedef struct pfsoft_server_stats {
     int queued, running;            /* right now */
 } pfsoft_server_stats;
 int pfsoft_server_create(size_t budget_bytes, int max_batch, int streams, pfsoft_server** out);
+/* As pfsoft_server_create, with flags. PFSOFT_SERVER_SPLIT: a batch takes waiting requests of one
+ * direction and ANY bandwidths (1 <= B <= 256; larger ones are rejected with PFSOFT_EINVAL) and runs
+ * their discrete Wigner transforms in one split-precision launch (the arithmetic of
+ * PFSOFT_BATCH_SPLIT; FFT passes per bandwidth). A request's workspace then also holds its
+ * operand-scale table (pfsoft_workspace_bytes(B) plus (4B(B+1) + B) * 16 bytes). A
+ * bounded wait that ran out finishes that batch's requests with PFSOFT_ETIMEOUT. */
+#define PFSOFT_SERVER_SPLIT 1
+int pfsoft_server_create_ex(size_t budget_bytes, int max_batch, int streams, int flags, pfsoft_server** out);
 int pfsoft_server_destroy(pfsoft_server* srv);
 int pfsoft_server_submit(pfsoft_server* srv, int direction, int B, const double* d_in, double* d_out, void* stream,
                          long long* id);
@@ -263,6 +272,12 @@ long long pfsoft_launch_count(void);
 /* Tuning knob used by the autotuner: direction 0 = DSOFT, 1 = IDSOFT; case_split 1 = each warp
  * applies all eight symmetry cases, 2 = warp pairs split them, 0 = library default. */
 int pfsoft_tune_dwt_case_split(int direction, int case_split);
+/* Test knob for the split-precision DWT's failure path (no counterpart in the reference): when
+ * wait_ns > 0, every later split launch first waits up to wait_ns nanoseconds on a barrier that
+ * nothing signals, before it issues any MMA; the wait runs out, every warp of the kernel leaves,
+ * the tensor memory is freed and pfsoft_batch_status then reports PFSOFT_ETIMEOUT. 0 restores
+ * normal operation. */
+int pfsoft_test_split_wait_ns(unsigned long long wait_ns);
 int pfsoft_profile_enable(int on);
 int pfsoft_profile_read(double* ms, long long* launches, int max_stages);
 const char* pfsoft_profile_stage_name(int stage);

@@ -5,7 +5,8 @@
 //               gridDim.z = transforms of the group]
 //   all groups: one persistent DWT launch over every (group, order class, transform block)
 //               item, longest first (dwt_batch.cu)
-// and the inverse runs the mirror image. Groups above B = 128 run the per-transform DWT kernels.
+// and the inverse runs the mirror image. FP64 groups above B = 128 run the per-transform DWT
+// kernels; with PFSOFT_BATCH_SPLIT every group up to B = 256 shares one split-precision launch.
 // The whole sequence is captured once into a CUDA graph; the device tables of grid and
 // coefficient pointers that the kernels read are refreshed before each replay, so one graph
 // serves any buffers.
@@ -200,11 +201,12 @@ struct pfsoft_batch {
     DwtItem* d_items = nullptr;
     int n_items = 0;
     int* d_counter = nullptr;
-    // split-precision DWT (PFSOFT_BATCH_SPLIT): items of the groups it takes, its counter and
-    // the sticky status of its bounded waits
+    // split-precision DWT (PFSOFT_BATCH_SPLIT): segments of the groups it takes (one per group),
+    // their item counts, and the sticky status of its bounded waits
     void* d_split_fwd = nullptr;
     void* d_split_inv = nullptr;
     int n_split_fwd = 0, n_split_inv = 0;
+    int n_split_seg = 0;
     int* d_split = nullptr;   // [0] counter, [1] status
     void* ws = nullptr;
     size_t ws_bytes = 0;
@@ -244,13 +246,14 @@ int enqueue(pfsoft_batch* b, int dir, cudaStream_t s)
         }
         for (const auto& g : b->groups)
             if (e == cudaSuccess && g.split)
-                e = dwt_split_scales(0, g.B, (int)g.members.size(), b->ws_ptrs() + g.ptr_base, b->coef_ptrs() + g.ptr_base, s);
+                e = dwt_split_scales(0, g.B, (int)g.members.size(), b->ws_ptrs() + g.ptr_base, b->coef_ptrs() + g.ptr_base, g.tables.w, s);
         if (e == cudaSuccess && b->n_split_fwd > 0) {
             e = cudaMemsetAsync(b->d_split, 0, sizeof(int), s);
-            if (e == cudaSuccess) e = dwt_split_launch(0, b->d_groups_fwd, b->d_split_fwd, b->n_split_fwd, b->d_split, b->d_split + 1, s);
+            if (e == cudaSuccess)
+                e = dwt_split_launch(0, b->d_groups_fwd, b->d_split_fwd, b->n_split_seg, b->n_split_fwd, b->d_split + 1, s);
         }
         for (const auto& g : b->groups)
-            if (e == cudaSuccess && g.B > kBatchMaxFused) e = dwt_large(g);
+            if (e == cudaSuccess && g.B > kBatchMaxFused && !g.split) e = dwt_large(g);
     } else {
         for (const auto& g : b->groups)
             if (e == cudaSuccess) e = zero_nyquist_launch(b->ws_ptrs() + g.ptr_base, g.B, (int)g.members.size(), s);
@@ -260,13 +263,14 @@ int enqueue(pfsoft_batch* b, int dir, cudaStream_t s)
         }
         for (const auto& g : b->groups)
             if (e == cudaSuccess && g.split)
-                e = dwt_split_scales(1, g.B, (int)g.members.size(), b->ws_ptrs() + g.ptr_base, b->coef_ptrs() + g.ptr_base, s);
+                e = dwt_split_scales(1, g.B, (int)g.members.size(), b->ws_ptrs() + g.ptr_base, b->coef_ptrs() + g.ptr_base, g.tables.w, s);
         if (e == cudaSuccess && b->n_split_inv > 0) {
             e = cudaMemsetAsync(b->d_split, 0, sizeof(int), s);
-            if (e == cudaSuccess) e = dwt_split_launch(1, b->d_groups_inv, b->d_split_inv, b->n_split_inv, b->d_split, b->d_split + 1, s);
+            if (e == cudaSuccess)
+                e = dwt_split_launch(1, b->d_groups_inv, b->d_split_inv, b->n_split_seg, b->n_split_inv, b->d_split + 1, s);
         }
         for (const auto& g : b->groups)
-            if (e == cudaSuccess && g.B > kBatchMaxFused) e = dwt_large(g);
+            if (e == cudaSuccess && g.B > kBatchMaxFused && !g.split) e = dwt_large(g);
         for (const auto& g : b->groups)
             if (e == cudaSuccess) e = fft_group(g, true);
         for (const auto& g : b->groups)
@@ -322,7 +326,7 @@ int pfsoft_batch_create(const int* bandwidths, int count, int transforms_per_cta
         g.members = kv.second;
         g.ptr_base = base;
         base += g.members.size();
-        g.split = (flags & PFSOFT_BATCH_SPLIT) && g.B <= kBatchMaxFused && dwt_split_supported(g.B);
+        g.split = (flags & PFSOFT_BATCH_SPLIT) && dwt_split_supported(g.B);
         for (int t : g.members) {
             ws_off[t] = ws_total;
             ws_total += ((size_t)g.N * g.N * g.N + (g.split ? dwt_split_aux_elems(g.B) : 0)) * sizeof(double2);
@@ -332,7 +336,7 @@ int pfsoft_batch_create(const int* bandwidths, int count, int transforms_per_cta
             free_batch(b);
             return rc;
         }
-        if (g.B <= kBatchMaxFused) b->nmax = std::max(b->nmax, g.N);
+        if (g.B <= kBatchMaxFused && !g.split) b->nmax = std::max(b->nmax, g.N);
         b->groups.push_back(g);
     }
     b->tpc = transforms_per_cta ? transforms_per_cta : dwt_batch_transforms_per_cta(std::max(b->nmax, 2));
@@ -342,22 +346,16 @@ int pfsoft_batch_create(const int* bandwidths, int count, int transforms_per_cta
     std::vector<DwtGroup> dg_f, dg_i;
     int gi_fused = 0;
     std::vector<int> fused_index(b->groups.size(), -1);
-    std::vector<unsigned char> split_f, split_i;   // forward items, then inverse items
-    int n_split_f = 0, n_split_i = 0;
+    std::vector<int> split_group, split_B, split_T;   // the split groups: index in d_groups, B, T
     for (size_t gi = 0; gi < b->groups.size(); ++gi) {
         const auto& g = b->groups[gi];
-        if (g.B > kBatchMaxFused) continue;
+        if (g.B > kBatchMaxFused && !g.split) continue;
         fused_index[gi] = gi_fused++;
         const int T = (int)g.members.size();
         if (g.split) {
-            std::vector<unsigned char> v;
-            int n = 0;
-            dwt_split_items(0, fused_index[gi], g.B, T, v, &n);
-            split_f.insert(split_f.end(), v.begin(), v.end());
-            n_split_f += n;
-            dwt_split_items(1, fused_index[gi], g.B, T, v, &n);
-            split_i.insert(split_i.end(), v.begin(), v.end());
-            n_split_i += n;
+            split_group.push_back(fused_index[gi]);
+            split_B.push_back(g.B);
+            split_T.push_back(T);
             continue;
         }
         for (int c = 0; c < num_classes(g.B); ++c) {
@@ -374,6 +372,9 @@ int pfsoft_batch_create(const int* bandwidths, int count, int transforms_per_cta
             }
         }
     }
+    std::vector<unsigned char> split_f, split_i;   // forward / inverse segments
+    const int n_split_f = dwt_split_segments(0, split_group, split_B, split_T, split_f);
+    const int n_split_i = dwt_split_segments(1, split_group, split_B, split_T, split_i);
     std::vector<int> order(items.size());
     for (size_t i = 0; i < order.size(); ++i) order[i] = (int)i;
     std::stable_sort(order.begin(), order.end(), [&](int x, int y) { return cost[x] > cost[y]; });
@@ -396,6 +397,7 @@ int pfsoft_batch_create(const int* bandwidths, int count, int transforms_per_cta
     }
     b->n_split_fwd = n_split_f;
     b->n_split_inv = n_split_i;
+    b->n_split_seg = (int)split_group.size();
     e = cudaMemset(b->d_split, 0, 2 * sizeof(int));
     if (e == cudaSuccess && (n_split_f > 0 || n_split_i > 0)) e = dwt_split_prepare();
     if (e == cudaSuccess && n_split_f > 0) e = cudaMemcpy(b->d_split_fwd, split_f.data(), split_f.size(), cudaMemcpyHostToDevice);
@@ -461,6 +463,12 @@ int pfsoft_batch_transforms_per_cta(const pfsoft_batch* b) { return b ? b->tpc :
 
 int pfsoft_split_supported(int B) { return dwt_split_supported(B) ? 1 : 0; }
 
+int pfsoft_test_split_wait_ns(unsigned long long wait_ns)
+{
+    dwt_split_set_fail_ns(wait_ns);
+    return PFSOFT_OK;
+}
+
 int pfsoft_batch_status(pfsoft_batch* b)
 {
     if (!b) return fail(PFSOFT_EINVAL, "null batch");
@@ -495,7 +503,7 @@ static int batch_run(pfsoft_batch* b, int dir, const double* const* in, double* 
     if (e == cudaSuccess) e = cudaEventRecord(b->uploaded, s);
     if (e != cudaSuccess) return fail(PFSOFT_ECUDA, std::string("pointer upload: ") + cudaGetErrorString(e));
     bool large = false;
-    for (const auto& g : b->groups) large |= g.B > kBatchMaxFused;
+    for (const auto& g : b->groups) large |= g.B > kBatchMaxFused && !g.split;
     // groups above the fused limit take their per-transform pointers at enqueue time, so they
     // are launched directly; everything else replays one captured graph
     if (!b->use_graph || large) {

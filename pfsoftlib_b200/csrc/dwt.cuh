@@ -104,20 +104,26 @@ cudaError_t dwt_batch_launch(int direction, const DwtGroup* d_groups, const DwtI
                              int* d_counter, int tpc, int nmax, cudaStream_t stream);
 
 // Split-precision DWT on the tensor cores (dwt_split.cu) for groups whose bandwidth passes
-// dwt_split_supported. Items (opaque, dwt_split_items) of group index `group` in d_groups; one
-// persistent launch; *d_counter must be 0; a wait that ran out sets *d_status to 1.
+// dwt_split_supported. A launch covers several groups of d_groups, described by segments
+// (dwt_split_segments: group index, bandwidth and transform count of each); one persistent
+// launch per direction; a bounded wait that ran out sets *d_status to 1.
 bool dwt_split_supported(int B);
-void dwt_split_items(int direction, int group, int B, int T, std::vector<unsigned char>& out, int* n_items);
-size_t dwt_split_item_bytes();
-cudaError_t dwt_split_prepare();   // kernel attributes; call once before any capture
+int dwt_split_segments(int direction, const std::vector<int>& group, const std::vector<int>& B,
+                       const std::vector<int>& T, std::vector<unsigned char>& out);   // returns the item count
+size_t dwt_split_seg_bytes();
+cudaError_t dwt_split_prepare();   // kernel attributes; call once per device before any capture
 // The split kernels read operand scales from a table of dwt_split_aux_elems(B) double2 that
 // follows each transform's spectrum (N^3 double2) in its workspace; dwt_split_scales fills it
-// (forward: from the spectra, after the FFT passes; inverse: from the coefficients).
+// (forward: from the spectra, after the FFT passes; inverse: from the coefficients), and the
+// row scales of the generated operand. w: the group's quadrature weights.
 size_t dwt_split_aux_elems(int B);
 cudaError_t dwt_split_scales(int direction, int B, int T, double2* const* d_ws, const double2* const* d_coeffs,
-                             cudaStream_t stream);
-cudaError_t dwt_split_launch(int direction, const DwtGroup* d_groups, const void* d_items, int n_items, int* d_counter,
+                             const double* w, cudaStream_t stream);
+cudaError_t dwt_split_launch(int direction, const DwtGroup* d_groups, const void* d_segs, int nseg, int n_items,
                              int* d_status, cudaStream_t stream);
+// Test knob: when nonzero, every later split launch first waits up to `ns` nanoseconds on a
+// barrier that nothing signals, before any MMA is issued, so that its bounded-wait exit runs.
+void dwt_split_set_fail_ns(unsigned long long ns);
 
 // Sets the detail string returned by pfsoft_last_error() on the calling thread.
 void set_last_error(const char* msg);

@@ -1,36 +1,52 @@
-// Split-precision discrete Wigner transform on the 5th-generation tensor cores (sm_100a).
+// Split-precision discrete Wigner transform on the 5th-generation tensor cores (sm_100a), as
+// exact products of 8-bit digit planes.
 //
-// For one order class (M, M') and four transforms of one bandwidth the DWT is a real matrix
-// product (see dwt_batch.cu for the case/column conventions):
+// For one order class (M, M') and up to two transforms of one bandwidth the DWT is a real matrix
+// product (see dwt_batch.cu for the case / column conventions):
 //   forward  F[l][c] = sum_k D[l][k] S[k][c]     l = M..B-1, k = beta samples, c = (transform, case, re/im)
 //   inverse  S[k][c] = sum_l D[l][k] G[l][c]
-// D (the Wigner-d rows, generated on chip by the FP64 three-term recurrence as in the FP64
-// kernels) and S / G (FP64 data) are turned into fixed point and cut into six balanced 8-bit
-// digits each: with a per-row scale r_l for D and a per-column power-of-two scale s_c for the
-// other operand, x = round(v * scale * 2^47) = sum_i d_i 256^i, d_i in [-128, 127]. A digit is an
-// integer that bf16 holds exactly. Digit planes are multiplied on the tensor cores
-// (tcgen05.mma kind::f16, bf16 x bf16 -> f32 in tensor memory) and summed by significance
-// e = sigma_D + sigma_S (sigma = 0 for the top digit); the planes with e > 5 are dropped. A
-// product of two digit planes summed over K <= 256 is an integer below 2^22, so the f32
-// accumulators of e <= 3 (at most four such sums) are exact, and the rounding in e = 4, 5 sits
-// 2^-32 below the result. The epilogue reads the six accumulators back, adds the five correction
-// planes smallest first in FP64 and the leading plane last in one rounding, then undoes the
-// scales. FP64 stays for the seeds, the recurrence, the weights and that final sum.
+// D (the Wigner-d rows, generated on chip by the FP64 three-term recurrence of
+// include/PFSOFTlib_headers/fn_dwt.hpp:167-199, as in the FP64 kernels) and S / G (FP64 data)
+// are turned into 48-bit fixed point with a per-row scale for D and a per-column power-of-two
+// scale for the other operand: x = round(v * scale * 2^47) = sum_i d_i 256^(5-i), d_i in
+// [-128, 127] (one FMA against a magic constant leaves x + sum 128*256^i in the low 48 bits of
+// a double; each byte XOR 0x80 is a signed digit). Digit planes are multiplied with
+// tcgen05.mma kind::i8 (signed 8-bit x signed 8-bit -> exact S32 in tensor memory): plane s of
+// the generated operand times the concatenated planes 0..5-s of the data operand lands in
+// accumulator planes s..5 (significance e = s + t; the 15 products with e > 5 are dropped). A
+// plane product summed over any K <= 2^16 is exact, so every bandwidth up to 256 (K = 512) is
+// exact in the integer sums; the epilogue combines the six planes in FP64 (Horner in 2^-8,
+// smallest first) and undoes the scales. FP64 stays for the seeds, the recurrence, the weights
+// and that final sum.
 //
-// Layout: one CTA (8 warps) per SM holds all 512 tensor-memory columns; accumulator plane e of
-// the 64 output columns sits at columns 64e .. 64e+63, one row per lane. The K dimension is
-// cut into chunks of 32; a chunk's digit planes of D (A operand) and of S or G (B operand) are
-// written to shared memory by all threads, double buffered, and one thread issues the chunk's
-// MMAs; an mbarrier signalled by tcgen05.commit says when a buffer may be rewritten.
-//   A (forward, MN-major, rows l):  plane s, row r, beta k:  s*SA + (r/8)*PA + (k/8)*128 + (k%8)*16 + (r%8)*2
-//   A (inverse, K-major, rows k):   plane s, row m, degree j: s*SA + (j/8)*PA + (m/8)*128 + (m%8)*16 + (j%8)*2
-//   B (K-major, columns n = 64*s + c): (k/8)*PB + (n/8)*128 + (n%8)*16 + (k%8)*2
-// so that a 16-byte unit holds eight consecutive degrees of one beta column (A) or eight
-// consecutive K of one column (B): each thread writes whole units.
-// Every wait is bounded; a wait that runs out sets *status and the CTA leaves after freeing its
-// tensor memory.
-
-#include <cuda_bf16.h>
+// Work items, dealt to the persistent CTAs in snake order over one index space:
+//   forward  (class, transforms t0..t0+nt-1, row tile): 128 degrees (M dimension) x all beta
+//            (K, chunks of 32); a second row tile (degrees M+128 ..) runs the recurrence through
+//            the first 128 degrees without storing them.
+//   inverse  (class, transforms, beta tile): 128 beta (M dimension) x all degrees (K, chunks of 32).
+// The items are not listed: a launch gets one segment per bandwidth group (host:
+// dwt_split_segments, largest bandwidth first), and item i of a segment is class i / (pairs *
+// tiles) -- classes run longest first (M ascending) -- then transform pair, then tile.
+// One CTA of 12 warps per SM, roles fixed per warp:
+//   warp 0      issues the MMAs (one lane) into one of two accumulator sets in tensor memory;
+//   warps 1-3   loaders: the data operand of a chunk (spectrum bins or coefficients) to digit planes;
+//   warps 4-7   epilogue: read an accumulator set back (warp w reads lanes 32(w%4) ..), combine, store;
+//   warps 8-11  generators: the Wigner rows of a chunk to digit planes (forward: one warp per
+//               chunk of 32 beta columns, all rows; inverse: the four warps on the tile's 128 beta
+//               columns, 32 degrees per chunk).
+// Chunks move through a ring of shared-memory stages (full / empty mbarriers; empty is signalled by
+// tcgen05.commit), accumulator sets through accfull / accempty, so generation, loading, MMAs and the
+// epilogue of different chunks and items overlap. Every wait is bounded (%globaltimer); a wait that
+// runs out sets a CTA-wide abort flag, every role leaves, the MMA lane waits (bounded) for its
+// committed MMAs before the tensor memory is freed, and *status is set to 1.
+//
+// Operand layouts in shared memory (no swizzle; see tc_sm100.cuh), per stage and plane:
+//   A forward (MN-major, rows = degrees):  (r/16)*512 + (k/8)*128 + (k%8)*16 + (r%16)
+//   A inverse (K-major, rows = beta):      (m/8)*256 + (j/16)*128 + (m%8)*16 + (j%16)
+//   B both    (K-major, rows = columns):   (n/8)*256 + (k/16)*128 + (n%8)*16 + (k%16),
+//             plane t of the data operand at rows 16*nt*t .. (planes concatenated along N)
+// so that a generator lane writes whole 16-byte units of 16 consecutive degrees of its beta column,
+// and a loader lane 8-byte halves of 8 consecutive K of one column.
 
 #include <algorithm>
 #include <cstdint>
@@ -48,98 +64,85 @@ namespace {
 
 using namespace dwtk;
 
-constexpr int kTT = 4;                 // transforms per work item
-constexpr int kCols = 16 * kTT;        // output columns per digit plane
+constexpr int kNT = 2;                 // transforms per work item (at most)
 constexpr int kPlanes = 6;             // digits per operand
-constexpr int kKC = 32;                // K per chunk
-constexpr int kThreads = 256;
-constexpr int kGenWarps = 7;           // forward: warps 1-7 generate, warp 0 issues the MMAs
+constexpr int kKC = 32;                // K per chunk: one kind::i8 MMA
+constexpr int kStages = 6;             // operand ring
+constexpr int kAccSets = 2;
+constexpr int kAccStride = 256;        // tensor-memory columns between the two accumulator sets
 constexpr uint32_t kTmemCols = 512;
+constexpr int kThreads = 384;
+constexpr int kLoadWarp0 = 1, kLoadWarps = 3;
+constexpr int kEpiWarp0 = 4;
+constexpr int kGenWarp0 = 8, kGenWarps = 4;
 constexpr uint64_t kWaitNs = 2000000000ull;   // 2 s
 
-// Shared memory (bytes). Both directions use the same buffer sizes.
-constexpr int kPAk = 128 * 16 + 16;                 // K-major A (inverse): stride of 8-wide K groups
-constexpr int kSAk = (kKC / 8) * kPAk;              // K-major A: plane stride
-constexpr int kPAm = kKC * 16 + 16;                 // MN-major A (forward): stride of 8-row M groups
-constexpr int kSAm = (128 / 8) * kPAm;              // MN-major A: plane stride
-constexpr int kABuf = kPlanes * (kSAk > kSAm ? kSAk : kSAm);
-constexpr int kPB = kPlanes * kCols * 16 + 16;      // B: k-group stride
-constexpr int kBBuf = (kKC / 8) * kPB;
-constexpr int kOffA = 0;
-constexpr int kOffB = kOffA + 2 * kABuf;
-constexpr int kOffRc = kOffB + 2 * kBBuf;            // recurrence coefficients, 256 rows x 4 doubles
-constexpr int kOffRs = kOffRc + 256 * 4 * 8;         // row scale * 2^47 (256 doubles)
-constexpr int kOffIrs = kOffRs + 256 * 8;            // 1 / row scale (256 doubles)
-constexpr int kOffCs = kOffIrs + 256 * 8;            // column scale * 2^47 (64 doubles)
-constexpr int kOffIcs = kOffCs + kCols * 8;          // 1 / column scale (64 doubles)
-constexpr int kOffRed = kOffIcs + kCols * 8;         // reduction scratch (256 doubles)
-constexpr int kOffCk = kOffRed + 256 * 8;           // forward: recurrence state every 16 rows, [8][256] double2
-constexpr int kOffCkSc = kOffCk + 8 * 256 * 16;      // forward: scale count at those rows, [8][256] int8
-constexpr int kOffCb = kOffCkSc + 8 * 256;           // forward: cos(beta) per column (256 doubles)
-constexpr int kOffCase = kOffCb + 256 * 8;          // the item's symmetry cases (8 PairCase)
-constexpr int kOffMisc = kOffCase + 8 * 32;          // mbarriers, tmem address, item index
-constexpr int kSmemBytes = kOffMisc + 64;
+constexpr int kAPlane = 4096;                       // 128 rows x 32 bytes of K
+constexpr int kABytes = kPlanes * kAPlane;          // 24 KB
+constexpr int kBRows = 16 * kNT * kPlanes;          // 192
+constexpr int kBBytes = kBRows / 8 * 256;           // 6 KB
+constexpr int kStageBytes = kABytes + kBBytes;
+constexpr int kOffBar = kStages * kStageBytes;
+// mbarriers: full[kStages], empty[kStages], accfull[2], accempty[2], drain, never (test knob)
+constexpr int kBarFull = 0, kBarEmpty = kStages, kBarAccFull = 2 * kStages, kBarAccEmpty = 2 * kStages + kAccSets,
+              kBarDrain = 2 * kStages + 2 * kAccSets, kBarNever = kBarDrain + 1, kNumBars = kBarNever + 1;
+constexpr int kOffMisc = kOffBar + kNumBars * 8;    // tensor-memory address, abort flag
+constexpr int kSmemBytes = kOffMisc + 16;
+static_assert(kStageBytes % 1024 == 0, "stages stay 1 KB aligned");
 static_assert(kSmemBytes <= 227 * 1024, "shared memory");
-
-static_assert(kOffB % 16 == 0 && kABuf % 16 == 0 && kBBuf % 16 == 0, "operand buffers must stay 16-byte aligned");
-static_assert(sizeof(PairCase) <= 32, "case table entry");
+static_assert(16 * kNT * kPlanes <= kAccStride, "an accumulator set fits its column range");
 
 constexpr double kTwo47 = 140737488355328.0;        // 2^47
 // 2^52 + sum_{i<6} 128 * 256^i: adding it to x * 2^47 (|x| < 0.5) leaves round(x * 2^47) + C in
 // the low 48 bits of the double, C making every byte a digit plus 128.
 constexpr double kMagic = 4503599627370496.0 + 141289400074368.0;
 
-struct SplitItem {
-    int group, cls, t0, nt, tile, pad0, pad1, pad2;
+// One bandwidth group of a launch: items first .. first+count-1, `pairs` transform pairs (T
+// transforms) and `tiles` tiles per class.
+struct SplitSeg {
+    int group, first, count, pairs, tiles, T, pad0, pad1;
 };
 
-// The six digits (most significant first) of the fixed-point value in a magic-biased double, as
-// bf16 bit patterns.
-__device__ __forceinline__ void to_digits(double z, uint16_t (&d)[kPlanes])
+// Digit words of four magic-biased values: w[p] holds byte (5 - p) of each value (value i in
+// byte i), XOR 0x80, i.e. plane p of the signed digits, most significant plane first.
+__device__ __forceinline__ void pack4(double z0, double z1, double z2, double z3, uint32_t (&w)[kPlanes])
 {
-    const unsigned long long bits = (unsigned long long)__double_as_longlong(z);
-    const uint32_t lo = (uint32_t)bits, hi = (uint32_t)(bits >> 32);
-    const uint32_t bias = 0x4B000000u;
-    uint32_t u[kPlanes];
-    asm("prmt.b32 %0, %1, %2, 0x7441;" : "=r"(u[0]) : "r"(hi), "r"(bias));   // byte 5
-    asm("prmt.b32 %0, %1, %2, 0x7440;" : "=r"(u[1]) : "r"(hi), "r"(bias));   // byte 4
-    asm("prmt.b32 %0, %1, %2, 0x7443;" : "=r"(u[2]) : "r"(lo), "r"(bias));   // byte 3
-    asm("prmt.b32 %0, %1, %2, 0x7442;" : "=r"(u[3]) : "r"(lo), "r"(bias));
-    asm("prmt.b32 %0, %1, %2, 0x7441;" : "=r"(u[4]) : "r"(lo), "r"(bias));
-    asm("prmt.b32 %0, %1, %2, 0x7440;" : "=r"(u[5]) : "r"(lo), "r"(bias));   // byte 0
-    // f = u - 128 exactly; an integer of at most 8 significant bits has zero low 16 bits in
-    // binary32, so its bf16 pattern is the high half
-#pragma unroll
-    for (int s = 0; s < kPlanes; ++s) {
-        const float f = __uint_as_float(u[s]) - 8388736.0f;   // 2^23 + 128
-        d[s] = (uint16_t)(__float_as_uint(f) >> 16);
-    }
+    const uint32_t L0 = (uint32_t)__double2loint(z0), H0 = (uint32_t)__double2hiint(z0);
+    const uint32_t L1 = (uint32_t)__double2loint(z1), H1 = (uint32_t)__double2hiint(z1);
+    const uint32_t L2 = (uint32_t)__double2loint(z2), H2 = (uint32_t)__double2hiint(z2);
+    const uint32_t L3 = (uint32_t)__double2loint(z3), H3 = (uint32_t)__double2hiint(z3);
+    const uint32_t a01 = tc::prmt(L0, L1, 0x5140), b01 = tc::prmt(L0, L1, 0x7362);
+    const uint32_t a23 = tc::prmt(L2, L3, 0x5140), b23 = tc::prmt(L2, L3, 0x7362);
+    const uint32_t h01 = tc::prmt(H0, H1, 0x5140), h23 = tc::prmt(H2, H3, 0x5140);
+    w[5] = tc::prmt(a01, a23, 0x5410) ^ 0x80808080u;   // byte 0
+    w[4] = tc::prmt(a01, a23, 0x7632) ^ 0x80808080u;   // byte 1
+    w[3] = tc::prmt(b01, b23, 0x5410) ^ 0x80808080u;   // byte 2
+    w[2] = tc::prmt(b01, b23, 0x7632) ^ 0x80808080u;   // byte 3
+    w[1] = tc::prmt(h01, h23, 0x5410) ^ 0x80808080u;   // byte 4
+    w[0] = tc::prmt(h01, h23, 0x7632) ^ 0x80808080u;   // byte 5
 }
 
-// Digits of eight values that share a 16-byte core-matrix unit (eight consecutive K or MN
-// positions of one row), one 32-bit word per two values and plane.
-struct Digits8 {
-    uint32_t w[kPlanes][4];
-};
-
-__device__ __forceinline__ void put_digits(Digits8& D, int j, double z)
+// 16 magic-biased values -> one 16-byte unit per plane at base + p * plane_stride
+__device__ __forceinline__ void store_unit16(unsigned char* base, int plane_stride, const double (&z)[16])
 {
-    uint16_t d[kPlanes];
-    to_digits(z, d);
+    uint32_t w0[kPlanes], w1[kPlanes], w2[kPlanes], w3[kPlanes];
+    pack4(z[0], z[1], z[2], z[3], w0);
+    pack4(z[4], z[5], z[6], z[7], w1);
+    pack4(z[8], z[9], z[10], z[11], w2);
+    pack4(z[12], z[13], z[14], z[15], w3);
 #pragma unroll
-    for (int s = 0; s < kPlanes; ++s) {
-        if (j & 1)
-            D.w[s][j >> 1] |= (uint32_t)d[s] << 16;
-        else
-            D.w[s][j >> 1] = d[s];
-    }
+    for (int p = 0; p < kPlanes; ++p)
+        *reinterpret_cast<uint4*>(base + p * plane_stride) = make_uint4(w0[p], w1[p], w2[p], w3[p]);
 }
 
-__device__ __forceinline__ void store_unit8(unsigned char* base, int plane_stride, const Digits8& D)
+// 8 magic-biased values -> one 8-byte half unit per plane
+__device__ __forceinline__ void store_unit8(unsigned char* base, int plane_stride, const double (&z)[8])
 {
+    uint32_t w0[kPlanes], w1[kPlanes];
+    pack4(z[0], z[1], z[2], z[3], w0);
+    pack4(z[4], z[5], z[6], z[7], w1);
 #pragma unroll
-    for (int s = 0; s < kPlanes; ++s)
-        *reinterpret_cast<uint4*>(base + s * plane_stride) = make_uint4(D.w[s][0], D.w[s][1], D.w[s][2], D.w[s][3]);
+    for (int p = 0; p < kPlanes; ++p) *reinterpret_cast<uint2*>(base + p * plane_stride) = make_uint2(w0[p], w1[p]);
 }
 
 // scale * 2^47 for a column whose largest magnitude is m (|v * scale| < 0.5), and 1 / scale
@@ -156,462 +159,435 @@ __device__ __forceinline__ void column_scale(double m, double& cs47, double& ics
     ics = ldexp(1.0, e + 1);
 }
 
-// Issues the MMAs of one K-step of 16: A plane s times the B planes 0 .. 5-s into accumulator
-// planes s .. 5 (tensor-memory columns 64s ..), pieces of at most 256 columns.
-__device__ __forceinline__ void issue_kstep(uint32_t tmem, uint32_t a_base, int a_plane, uint32_t a_lbo, uint32_t a_sbo,
-                                            bool a_mn, uint32_t b_base, bool first, int M = 128)
+// Item geometry shared by every role.
+struct ItemGeo {
+    const DwtGroup* gr;
+    int B, N, M, Mp, R, nc, t0, nt, tile, cls, nchunks;
+};
+
+// Geometry of item i: its segment by a scan over the launch's few segments, then class,
+// transform pair and tile. A forward row tile past the class's last degree has no chunks (every
+// role skips it alike).
+template <int DIR>
+__device__ __forceinline__ ItemGeo item_geo(const DwtGroup* __restrict__ groups, const SplitSeg* __restrict__ segs,
+                                            int nseg, int i)
 {
-#pragma unroll
-    for (int s = 0; s < kPlanes; ++s) {
-        const int total = kCols * (kPlanes - s);
-#pragma unroll
-        for (int n0 = 0; n0 < total; n0 += 256) {
-            const int n = total - n0 < 256 ? total - n0 : 256;
-            const uint64_t ad = tc::sdesc(a_base + s * a_plane, a_lbo, a_sbo);
-            const uint64_t bd = tc::sdesc(b_base + (n0 / 8) * 128, kPB, 128);
-            tc::mma_bf16(tmem + kCols * s + n0, ad, bd, tc::idesc_bf16(M, n, a_mn, false), !(first && s == 0));
-        }
-    }
+    int sidx = 0;
+    while (sidx + 1 < nseg && i >= segs[sidx + 1].first) ++sidx;
+    const SplitSeg sg = segs[sidx];
+    const int j = i - sg.first;
+    const int per_cls = sg.pairs * sg.tiles;
+    const int cls = j / per_cls, rem = j - cls * per_cls;
+    const int pair = rem / sg.tiles;
+    ItemGeo g;
+    g.gr = groups + sg.group;
+    g.B = g.gr->B;
+    g.N = g.gr->N;
+    class_orders(cls, g.M, g.Mp);
+    g.R = g.B - g.M;
+    g.nc = class_case_count(g.M, g.Mp);
+    g.t0 = kNT * pair;
+    g.nt = min(kNT, sg.T - g.t0);
+    g.tile = rem - pair * sg.tiles;
+    g.cls = cls;
+    if (DIR == 0)
+        g.nchunks = 128 * g.tile < g.R ? (g.N + kKC - 1) / kKC : 0;
+    else
+        g.nchunks = (g.R + kKC - 1) / kKC;
+    return g;
 }
 
-// One transform's 16 columns of row `lane` of this warp's lane quarter: planes combined in FP64.
-__device__ __forceinline__ void combine16(uint32_t taddr, int col, double (&out)[16])
+// The CTA's r-th item in snake order over the longest-first list (-1 past the end).
+__device__ __forceinline__ int cta_item(int r, int n_items)
 {
-    float v[16];
-    double corr[16];
-#pragma unroll
-    for (int j = 0; j < 16; ++j) corr[j] = 0.0;
-#pragma unroll
-    for (int e = kPlanes - 1; e >= 1; --e) {
-        tc::tmem_ld16(taddr + kCols * e + col, v);
-        tc::tmem_wait_ld();
-        const double w = ldexp(1.0, -14 - 8 * e);
-#pragma unroll
-        for (int j = 0; j < 16; ++j) corr[j] = fma((double)v[j], w, corr[j]);
-    }
-    tc::tmem_ld16(taddr + col, v);
-    tc::tmem_wait_ld();
-#pragma unroll
-    for (int j = 0; j < 16; ++j) out[j] = fma((double)v[j], 0x1p-14, corr[j]);
+    const int G = gridDim.x, b = blockIdx.x;
+    const int i = r * G + ((r & 1) ? (G - 1 - b) : b);
+    return i < n_items ? i : -1;
 }
 
-__device__ __forceinline__ double block_max(double v, double* red, int tid)
+// Row table of a transform's operand-scale area: {scale * 2^47, 1 / scale} per degree l.
+__device__ __forceinline__ const double2* row_table(const DwtGroup* gr, int t)
 {
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
-    if ((tid & 31) == 0) red[tid >> 5] = v;
-    __syncthreads();
-    double m = red[0];
-#pragma unroll
-    for (int w = 1; w < kThreads / 32; ++w) m = fmax(m, red[w]);
-    __syncthreads();
-    return m;
+    const int N = gr->N, B = gr->B;
+    const size_t a0 = (size_t)N * N > (size_t)8 * num_classes(B) ? (size_t)N * N : (size_t)8 * num_classes(B);
+    return gr->X[t] + (size_t)N * N * N + a0;
+}
+
+// One recurrence step of a beta column (fn_dwt.hpp:167-199): d(l+1) = d(l)(f1 f2 + f1 cos b) + c1 d(l-1);
+// a column whose seed was scaled by 2^600 rescales once it grows past 2^300 (and stores 0 meanwhile).
+__device__ __forceinline__ void rec_step(double& dcur, double& dprev, int& sc, double cb, double2 cf, double f1)
+{
+    const double t = fma(f1, cb, cf.y);
+    const double u = cf.x * dprev;
+    const double nx = fma(dcur, t, u);
+    dprev = dcur;
+    dcur = nx;
+    if (sc && fabs(dcur) >= 0x1p300) {
+        dcur *= 0x1p-600;
+        dprev *= 0x1p-600;
+        --sc;
+    }
 }
 
 template <int DIR>
-__global__ void __launch_bounds__(kThreads, 1) dwt_split_kernel(const DwtGroup* __restrict__ groups,
-                                                                 const SplitItem* __restrict__ items, int n_items,
-                                                                 int* __restrict__ counter, int* __restrict__ status)
+__global__ void __launch_bounds__(kThreads, 1)
+    dwt_split_kernel(const DwtGroup* __restrict__ groups, const SplitSeg* __restrict__ segs, int nseg, int n_items,
+                     int* __restrict__ status, unsigned long long fail_ns)
 {
     extern __shared__ __align__(1024) unsigned char smem[];
-    double* s_rc = reinterpret_cast<double*>(smem + kOffRc);
-    double* s_rs = reinterpret_cast<double*>(smem + kOffRs);
-    double* s_irs = reinterpret_cast<double*>(smem + kOffIrs);
-    double* s_cs = reinterpret_cast<double*>(smem + kOffCs);
-    double* s_ics = reinterpret_cast<double*>(smem + kOffIcs);
-    double* s_red = reinterpret_cast<double*>(smem + kOffRed);
-    uint64_t* s_mbar = reinterpret_cast<uint64_t*>(smem + kOffMisc);        // [2]
-    uint32_t* s_taddr = reinterpret_cast<uint32_t*>(smem + kOffMisc + 16);
-    int* s_item = reinterpret_cast<int*>(smem + kOffMisc + 20);
-    int* s_fail = reinterpret_cast<int*>(smem + kOffMisc + 24);
-
+    uint64_t* bars = reinterpret_cast<uint64_t*>(smem + kOffBar);
+    uint32_t* s_taddr = reinterpret_cast<uint32_t*>(smem + kOffMisc);
+    volatile int* s_abort = reinterpret_cast<volatile int*>(smem + kOffMisc + 4);
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+
     if (warp == 0) {
         tc::tmem_alloc(s_taddr, kTmemCols);
         tc::tmem_relinquish();
     }
-    if (tid == 0) {
-        tc::mbar_init(&s_mbar[0], 1);
-        tc::mbar_init(&s_mbar[1], 1);
+    if (tid == 32) {
+        for (int s = 0; s < kStages; ++s) {
+            tc::mbar_init(&bars[kBarFull + s], DIR == 0 ? 2 : 1 + kGenWarps);   // generator warp(s) + loader warp
+            tc::mbar_init(&bars[kBarEmpty + s], 1);                           // tcgen05.commit
+        }
+        for (int a = 0; a < kAccSets; ++a) {
+            tc::mbar_init(&bars[kBarAccFull + a], 1);
+            tc::mbar_init(&bars[kBarAccEmpty + a], 4);   // the four epilogue warps
+        }
+        tc::mbar_init(&bars[kBarDrain], 1);
+        tc::mbar_init(&bars[kBarNever], 1);
         tc::mbar_fence_init();
-        *s_fail = 0;
+        *s_abort = 0;
     }
     tc::fence_before_sync();
     __syncthreads();
     tc::fence_after_sync();
     const uint32_t tmem = *s_taddr;
     const uint32_t smem_base = tc::smem_u32(smem);
-    int commits[2] = {0, 0};   // commits issued to each buffer's mbarrier (uniform over the CTA)
-    int chunk = 0;             // chunks issued by this CTA
-    bool ok = true;
 
-    auto wait_buffer = [&](int b) -> bool {   // the MMAs of the buffer's last chunk have finished
-        if (commits[b] == 0) return true;
-        return tc::mbar_wait_bounded(&s_mbar[b], (uint32_t)((commits[b] - 1) & 1), kWaitNs);
-    };
-
-    // the recurrence step d(l+1) = d(l) (f1 f2 + f1 cos beta) + c1 d(l-1) (fn_dwt.hpp:167-199),
-    // ordered so that only one FMA depends on d(l); columns whose seed was scaled by 2^600 store 0
-    // until they are back in range
-    auto step = [&](double& dcur, double& dprev, int& sc, double cb, int r) {
-        const double2 ca = *reinterpret_cast<const double2*>(s_rc + 4 * r);
-        const double t = fma(s_rc[4 * r + 2], cb, ca.y);
-        const double u = ca.x * dprev;
-        const double nx = fma(dcur, t, u);
-        dprev = dcur;
-        dcur = nx;
-        if (sc && fabs(dcur) >= 0x1p300) {
-            dcur *= 0x1p-600;
-            dprev *= 0x1p-600;
-            --sc;
-        }
-    };
-
-    PairCase* s_case = reinterpret_cast<PairCase*>(smem + kOffCase);
-    int wgroup = -1;       // group whose largest weight is in wmax
-    double wmax = 0.0;
-    if (tid == kThreads - 1) *s_item = atomicAdd(counter, 1);
-    for (;;) {
-        __syncthreads();
-        const int idx = *s_item;
-        __syncthreads();
-        if (idx >= n_items) break;
-        // the next item, read after this one (the last warp has the least generation work)
-        if (tid == kThreads - 1) *s_item = atomicAdd(counter, 1);
-        const SplitItem it = items[idx];
-        const DwtGroup gr = groups[it.group];
-        const int B = gr.B, N = gr.N;
-        int M, Mp;
-        class_orders(it.cls, M, Mp);
-        const int nc = class_case_count(M, Mp);
-        const int R = B - M;   // degrees l = M .. B-1
-        const double nf = gr.normf[it.cls];
-
-        // recurrence coefficients of rows 0 .. R-1 (row r = degree M + r) and the row scales
-        if (DIR == 0 && it.group != wgroup) {
-            double w = 0.0;
-            for (int k = tid; k < N; k += kThreads) w = fmax(w, fabs(gr.w[k]));
-            wmax = block_max(w, s_red, tid);
-            wgroup = it.group;
-        }
-        const long long rc0 = rc_offset(B, M, Mp);
-        for (int r = tid; r < R; r += kThreads) {   // M + r < B: every row has a table entry
-            const double2 cf = __ldg(gr.rc_cf + rc0 + r);
-            s_rc[4 * r] = cf.x;
-            s_rc[4 * r + 1] = cf.y;
-            s_rc[4 * r + 2] = __ldg(gr.rc_f1 + rc0 + r);
-            const double bound = (DIR == 0 ? wmax : 1.0) * sqrt((double)(M + r) + 0.5);
-            const double rs = 0.49 / bound;
-            s_rs[r] = rs * kTwo47;
-            s_irs[r] = 1.0 / rs;
-        }
-        // column scales of the B operand: largest magnitudes precomputed per bin (forward) or per
-        // (class, case) (inverse) in the table past each transform's spectrum (dwt_split_scales)
-        if (tid < kCols / 2) {
-            const int t = tid >> 3, q = tid & 7;
-            double2 mx = make_double2(0.0, 0.0);
-            if (t < it.nt && q < nc) {
-                const double2* aux = gr.X[it.t0 + t] + (size_t)N * N * N;
-                if (DIR == 0) {
-                    const PairCase p = class_case(M, Mp, q, N);
-                    mx = aux[(size_t)p.row * N + p.col];
-                } else {
-                    mx = aux[(size_t)it.cls * 8 + q];
-                }
+    if (warp == 0) {
+        // ------------------------------------------------------------------ MMA issue
+        bool ok = true;
+        if (fail_ns) ok = tc::mbar_wait_bounded(&bars[kBarNever], 0, fail_ns, s_abort);   // test knob: nothing arrives
+        int g = 0, n = 0;   // chunks and (non-empty) items issued
+        for (int r = 0; ok; ++r) {
+            const int idx = cta_item(r, n_items);
+            if (idx < 0) break;
+            const ItemGeo it = item_geo<DIR>(groups, segs, nseg, idx);
+            if (it.nchunks == 0) continue;
+            const int a = n & 1, ua = n >> 1;
+            ++n;
+            if (!tc::mbar_wait_bounded(&bars[kBarAccEmpty + a], (uint32_t)((ua & 1) ^ 1), kWaitNs, s_abort)) {
+                ok = false;
+                break;
             }
-            column_scale(mx.x, s_cs[16 * t + 2 * q], s_ics[16 * t + 2 * q]);
-            column_scale(mx.y, s_cs[16 * t + 2 * q + 1], s_ics[16 * t + 2 * q + 1]);
-        }
-        if (tid < 8) s_case[tid] = class_case(M, Mp, tid < nc ? tid : 0, N);
-        __syncthreads();
-
-        if (DIR == 0) {
-            // ------------------------------------------------------------------ forward
-            // checkpoints: thread = beta column runs the recurrence over all rows once and keeps its
-            // state at every 16th row; each chunk then regenerates its rows 16 at a time
-            double2* s_ck = reinterpret_cast<double2*>(smem + kOffCk);
-            signed char* s_cksc = reinterpret_cast<signed char*>(smem + kOffCkSc);
-            double* s_cb = reinterpret_cast<double*>(smem + kOffCb);
-            // warps 1-7 regenerate rows in contiguous ranges of `rows` rows (a multiple of 8, so
-            // that a thread writes whole 16-byte units); warp 0 issues the MMAs
-            const int rows = (((R + kGenWarps - 1) / kGenWarps) + 7) & ~7;
-            if (tid < N) {
-                const int k = tid;
-                const double cb = gr.cosb[k];
-                s_cb[k] = cb;
-                int sc = 0;
-                double dcur = seed_value(nf * gr.w[k], gr.pw_sin[(size_t)(M - Mp) * N + k],
-                                         gr.pw_cos[(size_t)(M + Mp) * N + k], sc);
-                double dprev = 0.0;
-                for (int r = 0, g = 0, next = 0; r < R; ++r) {
-                    if (r == next) {
-                        s_ck[g * 256 + k] = make_double2(dcur, dprev);
-                        s_cksc[g * 256 + k] = (signed char)sc;
-                        ++g;
-                        next += rows;
+            tc::fence_after_sync();
+            const uint32_t dbase = tmem + (uint32_t)(a * kAccStride);
+            const int cols = 16 * it.nt;
+            for (int c = 0; c < it.nchunks; ++c, ++g) {
+                const int s = g % kStages, u = g / kStages;
+                if (!tc::mbar_wait_bounded(&bars[kBarFull + s], (uint32_t)(u & 1), kWaitNs, s_abort)) {
+                    ok = false;
+                    break;
+                }
+                tc::fence_after_sync();
+                if (lane == 0) {
+                    const uint32_t a0 = smem_base + s * kStageBytes, b0 = a0 + kABytes;
+                    const uint64_t bd = tc::sdesc(b0, 128, 256);
+#pragma unroll
+                    for (int p = 0; p < kPlanes; ++p) {
+                        const uint64_t ad = DIR == 0 ? tc::sdesc(a0 + p * kAPlane, 128, 512) : tc::sdesc(a0 + p * kAPlane, 128, 256);
+                        tc::mma_s8(dbase + (uint32_t)(cols * p), ad, bd, tc::idesc_s8(128, cols * (kPlanes - p), DIR == 0, false),
+                                   !(c == 0 && p == 0));
                     }
-                    step(dcur, dprev, sc, cb, r);
+                    tc::mma_commit(&bars[kBarEmpty + s]);
                 }
+                __syncwarp();
             }
-            // B operand tasks of the generating threads u = tid - 32: task e = u + 224 i is column
-            // n = e % 64 (transform n / 16, case (n / 2) % 8, re / im n % 2) at beta octet e / 64;
-            // its eight values are prefetched one chunk ahead
-            constexpr int kTasks = kCols * (kKC / 8);
-            constexpr int kSv = (kTasks + 32 * kGenWarps - 1) / (32 * kGenWarps);
-            double sv[kSv][8];
-            auto load_s = [&](int kc) {
-#pragma unroll
-                for (int i = 0; i < kSv; ++i) {
-                    const int e = (tid - 32) + 32 * kGenWarps * i;
-                    const int n = e & (kCols - 1), o = e / kCols;
-                    const int t = n >> 4, q = (n >> 1) & 7;
-                    const bool live = e < kTasks && t < it.nt && q < nc;
-                    const PairCase p = s_case[q];
-                    const double* col = live ? reinterpret_cast<const double*>(gr.X[it.t0 + t] + ((size_t)p.row * N + p.col) * N) + (n & 1)
-                                             : nullptr;
-#pragma unroll
-                    for (int j = 0; j < 8; ++j) {
-                        const int kk = kc * kKC + 8 * o + j;
-                        sv[i][j] = live ? __ldg(col + 2 * (p.rev ? N - 1 - kk : kk)) : 0.0;
+            if (!ok) break;
+            if (lane == 0) tc::mma_commit(&bars[kBarAccFull + a]);
+            __syncwarp();
+        }
+        // every MMA issued by this lane has completed before the tensor memory can be freed
+        if (lane == 0) {
+            tc::mma_commit(&bars[kBarDrain]);
+            const uint64_t t0 = tc::globaltimer_ns();
+            while (!tc::mbar_try_wait(&bars[kBarDrain], 0))
+                if (tc::globaltimer_ns() - t0 > kWaitNs) break;
+        }
+        __syncwarp();
+    } else if (warp >= kLoadWarp0 && warp < kLoadWarp0 + kLoadWarps) {
+        // ------------------------------------------------------------------ loaders (data operand)
+        const int L = warp - kLoadWarp0;
+        int g = 0;
+        for (int r = 0;; ++r) {
+            const int idx = cta_item(r, n_items);
+            if (idx < 0 || *s_abort) break;
+            const ItemGeo it = item_geo<DIR>(groups, segs, nseg, idx);
+            const int N = it.N, B = it.B, nt = it.nt;
+            if (DIR == 0 && lane < 16 && (g % kLoadWarps) == L) {
+                // the next item's bin columns into L2 while this one runs
+                const int nx = cta_item(r + 1, n_items);
+                if (nx >= 0) {
+                    const ItemGeo in = item_geo<DIR>(groups, segs, nseg, nx);
+                    const int t = lane >> 3, q = lane & 7;
+                    if (t < in.nt && q < in.nc) {
+                        const PairCase p = class_case(in.M, in.Mp, q, in.N);
+                        prefetch_l2(in.gr->X[in.t0 + t] + ((size_t)p.row * in.N + p.col) * in.N, (unsigned)in.N * 16u);
                     }
                 }
-            };
-            if (warp > 0) load_s(0);
-            __syncthreads();
-            const bool m64 = R <= 64;   // one M = 64 tile: rows 16q .. 16q+15 in lanes 32q .. 32q+15
-            const int gw = warp - 1;
-            const int r_lo = warp > 0 ? gw * rows : R, r_hi = min(r_lo + rows, (R + 7) & ~7);
-            const int nchunks = N / kKC;
-            for (int kc = 0; kc < nchunks; ++kc) {
-                const int b = chunk & 1;
-                if (tid == 0 && !wait_buffer(b)) ok = false;   // one waiter; the barrier below holds the rest
-                ok = !__syncthreads_or(!ok);
-                if (!ok) break;
-                unsigned char* A = smem + kOffA + b * kABuf;
-                unsigned char* Bm = smem + kOffB + b * kBBuf;
-                if (warp > 0) {
-                    // B operand: one 16-byte unit per plane for eight consecutive beta of column n
+            }
+            // per-lane column scales of the columns this lane converts: task e = lane + 32 i
+            // is (octet o = e % 4, column pair cp = e / 4 = 2 (case) + transform), i < 2 * nt
+            for (int c = 0; c < it.nchunks; ++c, ++g) {
+                if ((g % kLoadWarps) != L) continue;
+                const int s = g % kStages, u = g / kStages;
+                unsigned char* Bm = smem + s * kStageBytes + kABytes;
+                constexpr int kTasks = 8 * kNT * 4;   // column pairs x octets
+                double raw[kTasks / 32][8][2];
+                int tq[kTasks / 32], to[kTasks / 32];
+                // loads first (they fly while the stage is still being read by the MMAs)
 #pragma unroll
-                    for (int i = 0; i < kSv; ++i) {
-                        const int e = (tid - 32) + 32 * kGenWarps * i;
-                        if (e < kTasks) {
-                            const int n = e & (kCols - 1), o = e / kCols;
-                            Digits8 D;
+                for (int i = 0; i < kTasks / 32; ++i) {
+                    const int e = lane + 32 * i;
+                    const int o = e & 3, cpair = e >> 2;   // cpair = 8 t + q
+                    const int t = cpair >> 3, q = cpair & 7;
+                    tq[i] = cpair;
+                    to[i] = o;
+                    const bool live = t < nt && q < it.nc;
+                    if (DIR == 0) {
+                        const PairCase p = class_case(it.M, it.Mp, live ? q : 0, N);
+                        const double2* col = it.gr->X[it.t0 + (live ? t : 0)] + ((size_t)p.row * N + p.col) * N;
 #pragma unroll
-                            for (int j = 0; j < 8; ++j) put_digits(D, j, fma(sv[i][j], s_cs[n], kMagic));
-                            store_unit8(Bm + o * kPB + (n >> 3) * 128 + (n & 7) * 16, kCols * 16, D);
+                        for (int j = 0; j < 8; ++j) {
+                            const int k = c * kKC + 8 * o + j;
+                            double2 v = make_double2(0.0, 0.0);
+                            if (live && k < N) v = __ldg(col + (p.rev ? N - 1 - k : k));
+                            raw[i][j][0] = v.x;
+                            raw[i][j][1] = v.y;
+                        }
+                    } else {
+                        const PairCase p = class_case(it.M, it.Mp, live ? q : 0, N);
+                        const double2* cf = it.gr->coeffs[it.t0 + (live ? t : 0)];
+#pragma unroll
+                        for (int j = 0; j < 8; ++j) {
+                            const int l = it.M + c * kKC + 8 * o + j;
+                            double2 v = make_double2(0.0, 0.0);
+                            if (live && l < B) v = __ldg(cf + coef_index(l, p.m1, p.m2));
+                            raw[i][j][0] = v.x;
+                            raw[i][j][1] = v.y;
                         }
                     }
-                    if (kc + 1 < nchunks) load_s(kc + 1);   // in flight during the generation below
-                    // A operand (MN-major): thread = beta column lane of the chunk, rows r_lo .. r_hi-1
-                    // from the checkpoint, one 16-byte unit per plane for eight rows
-                    if (r_lo < r_hi) {
-                        const int k = kc * kKC + lane;
-                        const double cb = s_cb[k];
-                        const double2 st = s_ck[gw * 256 + k];
-                        int sc = s_cksc[gw * 256 + k];
-                        double dcur = st.x, dprev = st.y;
-                        unsigned char* colp = A + (lane >> 3) * 128 + (lane & 7) * 16;
-                        for (int r8 = r_lo; r8 < r_hi; r8 += 8) {
-                            Digits8 D;
+                }
+                if (!tc::mbar_wait_bounded(&bars[kBarEmpty + s], (uint32_t)((u & 1) ^ 1), kWaitNs, s_abort)) break;
 #pragma unroll
-                            for (int j = 0; j < 8; ++j) {
-                                const int r = r8 + j;
-                                if (r < R) {
-                                    put_digits(D, j, fma(sc ? 0.0 : dcur, s_rs[r], kMagic));
-                                    step(dcur, dprev, sc, cb, r);
+                for (int i = 0; i < kTasks / 32; ++i) {
+                    const int cpair = tq[i], o = to[i];
+                    const int t = cpair >> 3, q = cpair & 7;
+                    if (t >= nt || q >= it.nc) continue;   // columns never stored: left as they are
+                    const double2* aux = it.gr->X[it.t0 + t] + (size_t)N * N * N;
+                    double2 mx;
+                    double sgn_norm = 1.0;
+                    PairCase p = class_case(it.M, it.Mp, q, N);
+                    if (DIR == 0) {
+                        mx = aux[(size_t)p.row * N + p.col];
+                    } else {
+                        mx = aux[(size_t)it.cls * 8 + q];
+                        sgn_norm = (double)(B * 2 * B) / kPi;   // src/fn_idsoft.cpp:109
+                    }
+                    double cs_re, cs_im, ics_unused;
+                    column_scale(mx.x, cs_re, ics_unused);
+                    column_scale(mx.y, cs_im, ics_unused);
+                    double zr[8], zi[8];
+                    if (DIR == 0) {
+#pragma unroll
+                        for (int j = 0; j < 8; ++j) {
+                            zr[j] = fma(raw[i][j][0], cs_re, kMagic);
+                            zi[j] = fma(raw[i][j][1], cs_im, kMagic);
+                        }
+                    } else {
+                        // G = norm * sign(l) * f / (row scale), zero past the last degree
+                        const double2* rows = row_table(it.gr, it.t0);
+#pragma unroll
+                        for (int j = 0; j < 8; ++j) {
+                            const int l = it.M + c * kKC + 8 * o + j;
+                            double f = 0.0;
+                            if (l < B) f = sgn_norm * case_sign(p, l, it.M) * __ldg(&rows[l].y);
+                            zr[j] = fma(f * raw[i][j][0], cs_re, kMagic);
+                            zi[j] = fma(f * raw[i][j][1], cs_im, kMagic);
+                        }
+                    }
+                    const int n = 16 * t + 2 * q;   // re column; im is n + 1
+                    const int plane_rows = 16 * nt;
+                    // rows n, n+1 of plane 0; plane p at rows + 16 nt p: (n/8)*256 + (k/16)*128 + (n%8)*16 + k%16
+                    unsigned char* unit = Bm + (n >> 3) * 256 + (o >> 1) * 128 + (n & 7) * 16 + (o & 1) * 8;
+                    const int pstride = plane_rows / 8 * 256;
+                    store_unit8(unit, pstride, zr);
+                    store_unit8(unit + 16, pstride, zi);
+                }
+                tc::fence_proxy_async();
+                __syncwarp();
+                if (lane == 0) tc::mbar_arrive(&bars[kBarFull + s]);
+            }
+            if (*s_abort) break;
+        }
+    } else if (warp >= kEpiWarp0 && warp < kEpiWarp0 + 4) {
+        // ------------------------------------------------------------------ epilogue
+        const int q4 = warp & 3;   // tensor-memory lane quarter
+        int n = 0;
+        for (int r = 0;; ++r) {
+            const int idx = cta_item(r, n_items);
+            if (idx < 0) break;
+            const ItemGeo it = item_geo<DIR>(groups, segs, nseg, idx);
+            if (it.nchunks == 0) continue;
+            const int a = n & 1, ua = n >> 1;
+            ++n;
+            if (!tc::mbar_wait_bounded(&bars[kBarAccFull + a], (uint32_t)(ua & 1), kWaitNs, s_abort)) break;
+            tc::fence_after_sync();
+            const int N = it.N, B = it.B;
+            const int row = 32 * q4 + lane;
+            const uint32_t taddr = tmem + ((uint32_t)(32 * q4) << 16) + (uint32_t)(a * kAccStride);
+            const int cols = 16 * it.nt;
+            // forward: degree l of this lane; inverse: beta k
+            const int l = it.M + 128 * it.tile + row;
+            const int k = 128 * it.tile + row;
+            const bool live = DIR == 0 ? (l < B) : (k < N);
+            double rowf = 0.0;
+            if (DIR == 0 && live) rowf = (kPi / (double)(B * 2 * B)) * __ldg(&row_table(it.gr, it.t0)[l].y);   // src/fn_dsoft.cpp:119
+            for (int t = 0; t < it.nt; ++t) {
+                int32_t acc[kPlanes][16];
+#pragma unroll
+                for (int e = 0; e < kPlanes; ++e) tc::tmem_ld16(taddr + (uint32_t)(cols * e + 16 * t), acc[e]);
+                tc::tmem_wait_ld();
+                double v[16];
+#pragma unroll
+                for (int j = 0; j < 16; ++j) {
+                    double h = (double)acc[5][j];
+                    h = fma(h, 0x1p-8, (double)acc[4][j]);
+                    h = fma(h, 0x1p-8, (double)acc[3][j]);
+                    h = fma(h, 0x1p-8, (double)acc[2][j]);
+                    h = fma(h, 0x1p-8, (double)acc[1][j]);
+                    v[j] = fma(h, 0x1p-8, (double)acc[0][j]) * 0x1p-14;
+                }
+                if (!live) continue;
+                const double2* aux = it.gr->X[it.t0 + t] + (size_t)N * N * N;
+#pragma unroll
+                for (int q = 0; q < 8; ++q) {
+                    if (q >= it.nc) break;
+                    const PairCase p = class_case(it.M, it.Mp, q, N);
+                    const double2 mx = DIR == 0 ? aux[(size_t)p.row * N + p.col] : aux[(size_t)it.cls * 8 + q];
+                    double unused, ics_re, ics_im;
+                    column_scale(mx.x, unused, ics_re);
+                    column_scale(mx.y, unused, ics_im);
+                    if (DIR == 0) {
+                        const double f = rowf * case_sign(p, l, it.M);
+                        it.gr->coeffs[it.t0 + t][coef_index(l, p.m1, p.m2)] =
+                            make_double2(f * v[2 * q] * ics_re, f * v[2 * q + 1] * ics_im);
+                    } else {
+                        it.gr->X[it.t0 + t][((size_t)p.row * N + p.col) * N + (p.rev ? N - 1 - k : k)] =
+                            make_double2(v[2 * q] * ics_re, v[2 * q + 1] * ics_im);
+                    }
+                }
+            }
+            tc::fence_before_sync();
+            __syncwarp();
+            if (lane == 0) tc::mbar_arrive(&bars[kBarAccEmpty + a]);
+        }
+    } else if (warp >= kGenWarp0) {
+        // ------------------------------------------------------------------ generators (Wigner rows)
+        const int w = warp - kGenWarp0;
+        int g = 0;
+        for (int r = 0;; ++r) {
+            const int idx = cta_item(r, n_items);
+            if (idx < 0 || *s_abort) break;
+            const ItemGeo it = item_geo<DIR>(groups, segs, nseg, idx);
+            const int N = it.N;
+            const DwtGroup* gr = it.gr;
+            const long long rc0 = rc_offset(it.B, it.M, it.Mp);
+            const double nf = gr->normf[it.cls];
+            const double2* rows = row_table(gr, it.t0);
+            if (DIR == 0) {
+                // forward: this warp's chunks (beta columns 32c + lane), rows of the item's tile
+                const int r0 = 128 * it.tile, rn = min(it.R - r0, 128);
+                for (int c = 0; c < it.nchunks; ++c, ++g) {
+                    if ((g % kGenWarps) != w) continue;
+                    const int s = g % kStages, u = g / kStages;
+                    const int k = c * kKC + lane;
+                    double cb = 0.0, dcur = 0.0, dprev = 0.0;
+                    int sc = 0;
+                    if (k < N) {
+                        cb = gr->cosb[k];
+                        dcur = seed_value(nf * gr->w[k], gr->pw_sin[(size_t)(it.M - it.Mp) * N + k],
+                                          gr->pw_cos[(size_t)(it.M + it.Mp) * N + k], sc);
+                    }
+                    for (int rr = 0; rr < r0; ++rr)   // second row tile: run through the first 128 degrees
+                        rec_step(dcur, dprev, sc, cb, __ldg(gr->rc_cf + rc0 + rr), __ldg(gr->rc_f1 + rc0 + rr));
+                    if (!tc::mbar_wait_bounded(&bars[kBarEmpty + s], (uint32_t)((u & 1) ^ 1), kWaitNs, s_abort)) break;
+                    unsigned char* A = smem + s * kStageBytes + lane * 16;   // (k/8)*128 + (k%8)*16 = lane*16
+                    if (k < N) {
+                        for (int r16 = 0; r16 < rn; r16 += 16) {
+                            double z[16];
+#pragma unroll
+                            for (int j = 0; j < 16; ++j) {
+                                const int rr = r0 + r16 + j;
+                                if (rr < it.R) {
+                                    z[j] = fma(sc ? 0.0 : dcur, __ldg(&rows[it.M + rr].x), kMagic);
+                                    rec_step(dcur, dprev, sc, cb, __ldg(gr->rc_cf + rc0 + rr), __ldg(gr->rc_f1 + rc0 + rr));
                                 } else {
-                                    put_digits(D, j, kMagic);
+                                    z[j] = kMagic;
                                 }
                             }
-                            store_unit8(colp + (r8 >> 3) * kPAm, kSAm, D);
+                            store_unit16(A + (r16 >> 4) * 512, kAPlane, z);
                         }
                     }
+                    tc::fence_proxy_async();
+                    __syncwarp();
+                    if (lane == 0) tc::mbar_arrive(&bars[kBarFull + s]);
                 }
-                tc::fence_proxy_async();
-                tc::fence_before_sync();
-                __syncthreads();
-                if (tid == 0) {
-                    tc::fence_after_sync();
-                    const uint32_t a0 = smem_base + kOffA + b * kABuf, b0 = smem_base + kOffB + b * kBBuf;
-                    const int mt = m64 ? 64 : 128;
-                    issue_kstep(tmem, a0, kSAm, 128, kPAm, true, b0, kc == 0, mt);
-                    issue_kstep(tmem, a0 + 256, kSAm, 128, kPAm, true, b0 + 2 * kPB, false, mt);
-                    tc::mma_commit(&s_mbar[b]);
+            } else {
+                // inverse: beta column k of the tile for this lane, 32 degrees per chunk
+                const int m = 32 * w + lane;
+                const int k = 128 * it.tile + m;
+                double cb = 0.0, dcur = 0.0, dprev = 0.0;
+                int sc = 0;
+                if (k < N) {
+                    cb = gr->cosb[k];
+                    dcur = seed_value(nf, gr->pw_sin[(size_t)(it.M - it.Mp) * N + k], gr->pw_cos[(size_t)(it.M + it.Mp) * N + k], sc);
                 }
-                ++commits[b];
-                ++chunk;
-            }
-            if (!ok) break;
-            // epilogue: lane quarter warp % 4, transforms 2 (warp / 4) + {0, 1}
-            if (tid == 0 && !wait_buffer((chunk - 1) & 1)) ok = false;
-            ok = !__syncthreads_or(!ok);
-            if (!ok) break;
-            tc::fence_after_sync();
-            const int r = m64 ? (lane < 16 ? 16 * (warp & 3) + lane : 1 << 20) : 32 * (warp & 3) + lane;
-            const int l = M + r;
-            const uint32_t taddr = tmem + ((uint32_t)(32 * (warp & 3)) << 16);
-            const double norm = kPi / (double)(B * 2 * B);   // src/fn_dsoft.cpp:119
-            for (int tt = 0; tt < 2; ++tt) {
-                const int t = 2 * (warp >> 2) + tt;
-                double v[16];
-                combine16(taddr, 16 * t, v);
-                if (r < R && t < it.nt) {
-                    double2* out = gr.coeffs[it.t0 + t];
-                    const double irs = s_irs[r];
-#pragma unroll
-                    for (int q = 0; q < 8; ++q) {
-                        if (q < nc) {
-                            const PairCase p = s_case[q];
-                            const double f = norm * case_sign(p, l, M) * irs;
-                            out[coef_index(l, p.m1, p.m2)] =
-                                make_double2(f * v[2 * q] * s_ics[16 * t + 2 * q], f * v[2 * q + 1] * s_ics[16 * t + 2 * q + 1]);
-                        }
-                    }
-                }
-            }
-            tc::fence_before_sync();
-            __syncthreads();   // accumulators are overwritten by the next item
-        } else {
-            // ------------------------------------------------------------------ inverse
-            // warps 0-3 generate: thread = beta column m of the tile, rows advance over the chunks;
-            // warps 4-7 bring in the coefficients
-            const int kb = 128 * it.tile;
-            const int m = tid & 127, k = kb + m;
-            const bool gen = tid < 128;
-            double cb = 0.0, dcur = 0.0, dprev = 0.0;
-            int sc = 0;
-            if (gen && k < N) {
-                cb = gr.cosb[k];
-                dcur = seed_value(nf, gr.pw_sin[(size_t)(M - Mp) * N + k], gr.pw_cos[(size_t)(M + Mp) * N + k], sc);
-            }
-            const double norm = (double)(B * 2 * B) / kPi;   // src/fn_idsoft.cpp:109
-            const int nchunks = (R + kKC - 1) / kKC;
-            // B operand tasks of the loading threads u = tid - 160 (warps 5-7; warp 4 issues the
-            // MMAs): task e = u + 96 i is column n = e % 64 at row octet e / 64 of the chunk; its
-            // eight coefficients are prefetched one chunk ahead and signed and scaled when stored
-            constexpr int kTasks = kCols * (kKC / 8);
-            constexpr int kGv = (kTasks + 95) / 96;
-            const bool loader = tid >= 160;
-            double gv[kGv][8];
-            auto load_g = [&](int lc) {   // raw loads only, every address in range, so they all fly at once
-#pragma unroll
-                for (int i = 0; i < kGv; ++i) {
-                    const int e = min((tid - 160) + 96 * i, kTasks - 1);
-                    const int n = e & (kCols - 1), o = e / kCols;
-                    const int t = min(n >> 4, it.nt - 1), q = (n >> 1) & 7;
-                    const PairCase p = s_case[q];
-                    const double* cf = reinterpret_cast<const double*>(gr.coeffs[it.t0 + t]) + (n & 1);
-#pragma unroll
-                    for (int j = 0; j < 8; ++j) {
-                        const int l = M + min(lc * kKC + 8 * o + j, R - 1);
-                        gv[i][j] = __ldg(cf + 2 * coef_index(l, p.m1, p.m2));
-                    }
-                }
-            };
-            if (loader) load_g(0);
-            for (int lc = 0; lc < nchunks; ++lc) {
-                const int b = chunk & 1;
-                if (tid == 0 && !wait_buffer(b)) ok = false;   // one waiter; the barrier below holds the rest
-                ok = !__syncthreads_or(!ok);
-                if (!ok) break;
-                unsigned char* A = smem + kOffA + b * kABuf;
-                unsigned char* Bm = smem + kOffB + b * kBBuf;
-                const int r0 = lc * kKC;
-                if (gen) {
-                    // A operand (K-major): thread = beta column m of the tile, one 16-byte unit per
-                    // plane for eight consecutive rows
-                    unsigned char* colp = A + (m >> 3) * 128 + (m & 7) * 16;
+                for (int c = 0; c < it.nchunks; ++c, ++g) {
+                    const int s = g % kStages, u = g / kStages;
+                    if (!tc::mbar_wait_bounded(&bars[kBarEmpty + s], (uint32_t)((u & 1) ^ 1), kWaitNs, s_abort)) break;
+                    unsigned char* A = smem + s * kStageBytes + (m >> 3) * 256 + (m & 7) * 16;
 #pragma unroll 1
-                    for (int j8 = 0; j8 < kKC; j8 += 8) {
-                        Digits8 D;
+                    for (int h = 0; h < 2; ++h) {
+                        double z[16];
 #pragma unroll
-                        for (int jj = 0; jj < 8; ++jj) {
-                            const int r = r0 + j8 + jj;
-                            if (r < R && k < N) {
-                                put_digits(D, jj, fma(sc ? 0.0 : dcur, s_rs[r], kMagic));
-                                step(dcur, dprev, sc, cb, r);
+                        for (int j = 0; j < 16; ++j) {
+                            const int rr = c * kKC + 16 * h + j;
+                            if (rr < it.R) {
+                                z[j] = fma(sc ? 0.0 : dcur, __ldg(&rows[it.M + rr].x), kMagic);
+                                rec_step(dcur, dprev, sc, cb, __ldg(gr->rc_cf + rc0 + rr), __ldg(gr->rc_f1 + rc0 + rr));
                             } else {
-                                put_digits(D, jj, kMagic);
+                                z[j] = kMagic;
                             }
                         }
-                        store_unit8(colp + (j8 >> 3) * kPAk, kSAk, D);
+                        store_unit16(A + h * 128, kAPlane, z);
                     }
-                } else if (loader) {
-#pragma unroll
-                    for (int i = 0; i < kGv; ++i) {
-                        const int e = (tid - 160) + 96 * i;
-                        if (e < kTasks) {
-                            const int n = e & (kCols - 1), o = e / kCols;
-                            const int t = n >> 4, q = (n >> 1) & 7;
-                            const bool live = t < it.nt && q < nc;
-                            const PairCase p = s_case[q];
-                            Digits8 D;
-#pragma unroll
-                            for (int j = 0; j < 8; ++j) {
-                                // G = norm * sign * coefficient / (row scale), zero outside the class
-                                const int r = r0 + 8 * o + j, l = M + r;
-                                const double g = (live && r < R) ? norm * case_sign(p, l, M) * s_irs[r] * gv[i][j] : 0.0;
-                                put_digits(D, j, fma(g, s_cs[n], kMagic));
-                            }
-                            store_unit8(Bm + o * kPB + (n >> 3) * 128 + (n & 7) * 16, kCols * 16, D);
-                        }
-                    }
-                    if (lc + 1 < nchunks) load_g(lc + 1);
-                }
-                tc::fence_proxy_async();
-                tc::fence_before_sync();
-                __syncthreads();
-                if (tid == 128) {
-                    tc::fence_after_sync();
-                    const uint32_t a0 = smem_base + kOffA + b * kABuf, b0 = smem_base + kOffB + b * kBBuf;
-                    issue_kstep(tmem, a0, kSAk, kPAk, 128, false, b0, lc == 0);
-                    if (r0 + 16 < R) issue_kstep(tmem, a0 + 2 * kPAk, kSAk, kPAk, 128, false, b0 + 2 * kPB, false);
-                    tc::mma_commit(&s_mbar[b]);
-                }
-                ++commits[b];
-                ++chunk;
-            }
-            if (!ok) break;
-            if (tid == 0 && !wait_buffer((chunk - 1) & 1)) ok = false;
-            ok = !__syncthreads_or(!ok);
-            if (!ok) break;
-            tc::fence_after_sync();
-            // epilogue: row m = 32 (warp % 4) + lane of the tile, transforms 2 (warp / 4) + {0, 1}
-            const int mm = 32 * (warp & 3) + lane, kk = kb + mm;
-            const uint32_t taddr = tmem + ((uint32_t)(32 * (warp & 3)) << 16);
-            for (int tt = 0; tt < 2; ++tt) {
-                const int t = 2 * (warp >> 2) + tt;
-                double v[16];
-                combine16(taddr, 16 * t, v);
-                if (kk < N && t < it.nt) {
-                    double2* X = gr.X[it.t0 + t];
-#pragma unroll
-                    for (int q = 0; q < 8; ++q) {
-                        if (q < nc) {
-                            const PairCase p = s_case[q];
-                            X[((size_t)p.row * N + p.col) * N + (p.rev ? N - 1 - kk : kk)] =
-                                make_double2(v[2 * q] * s_ics[16 * t + 2 * q], v[2 * q + 1] * s_ics[16 * t + 2 * q + 1]);
-                        }
-                    }
+                    tc::fence_proxy_async();
+                    __syncwarp();
+                    if (lane == 0) tc::mbar_arrive(&bars[kBarFull + s]);
                 }
             }
-            tc::fence_before_sync();
-            __syncthreads();
+            if (*s_abort) break;
         }
     }
-    // leave: a failed wait may leave MMAs in flight; give them the same bound once more
-    if (!ok) {
-        if (tid == 0) {
-            *s_fail = 1;
-            atomicExch(status, 1);
-        }
-        if (tid == 0)
-            for (int b = 0; b < 2; ++b) wait_buffer(b);
-    }
+
     tc::fence_before_sync();
     __syncthreads();
-    if (warp == 0) tc::tmem_dealloc(tmem, kTmemCols);
+    if (*s_abort && tid == 0) atomicExch(status, 1);
+    if (warp == 0) {
+        tc::fence_after_sync();
+        tc::tmem_dealloc(tmem, kTmemCols);
+    }
 }
 
 // Largest |re|, |im| over beta of every bin column of a spectrum, into the table past it
@@ -661,20 +637,46 @@ __global__ void split_coefmax_kernel(double2* const* X, const double2* const* co
     X[blockIdx.z][(size_t)N * N * N + i] = make_double2(mre, mim);
 }
 
+// Row scales of the generated operand, {0.49 / bound * 2^47, bound / 0.49} per degree l, bound =
+// |d~^l| <= sqrt(l + 1/2) (times the largest weight for the forward's weighted rows), into the
+// row table of every transform of the group. One block per transform.
+__global__ void split_rows_kernel(double2* const* X, const double* w, int B, int weighted)
+{
+    __shared__ double red[8];
+    const int N = 2 * B;
+    double m = 0.0;
+    if (weighted)
+        for (int k = threadIdx.x; k < N; k += blockDim.x) m = fmax(m, fabs(w[k]));
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = m;
+    __syncthreads();
+    double wmax = 1.0;
+    if (weighted) {
+        wmax = red[0];
+        for (int i = 1; i < (int)(blockDim.x >> 5); ++i) wmax = fmax(wmax, red[i]);
+    }
+    const size_t a0 = (size_t)N * N > (size_t)8 * num_classes(B) ? (size_t)N * N : (size_t)8 * num_classes(B);
+    double2* rows = X[blockIdx.z] + (size_t)N * N * N + a0;
+    for (int l = threadIdx.x; l < B; l += blockDim.x) {
+        const double bound = wmax * sqrt((double)l + 0.5);
+        const double rs = 0.49 / bound;
+        rows[l] = make_double2(rs * kTwo47, 1.0 / rs);
+    }
+}
+
 }  // namespace
 
-bool dwt_split_supported(int B) { return B >= 16 && B <= 128 && B % 16 == 0; }
-
-size_t dwt_split_item_bytes() { return sizeof(SplitItem); }
+bool dwt_split_supported(int B) { return B >= 1 && B <= 256; }
 
 size_t dwt_split_aux_elems(int B)
 {
     const size_t n2 = (size_t)4 * B * B, c8 = (size_t)8 * num_classes(B);
-    return n2 > c8 ? n2 : c8;
+    return (n2 > c8 ? n2 : c8) + (size_t)B;
 }
 
 cudaError_t dwt_split_scales(int direction, int B, int T, double2* const* d_ws, const double2* const* d_coeffs,
-                             cudaStream_t s)
+                             const double* w, cudaStream_t s)
 {
     const int N = 2 * B;
     if (direction == 0) {
@@ -684,33 +686,43 @@ cudaError_t dwt_split_scales(int direction, int B, int T, double2* const* d_ws, 
         dim3 grid((unsigned)((num_classes(B) * 8 + 255) / 256), 1, (unsigned)T);
         split_coefmax_kernel<<<grid, 256, 0, s>>>(d_ws, d_coeffs, B);
     }
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    split_rows_kernel<<<dim3(1, 1, (unsigned)T), 256, 0, s>>>(d_ws, w, B, direction == 0 ? 1 : 0);
     return cudaGetLastError();
 }
 
-// Work items of one group for the split kernel: forward (class, 4 transforms), inverse (class,
-// 128 beta columns, 4 transforms); longest first.
-void dwt_split_items(int direction, int group, int B, int T, std::vector<unsigned char>& out, int* n_items)
+// Segments of a launch over several groups (group index, bandwidth and transform count each),
+// largest bandwidth first; returns the number of items. Forward: 128-degree row tiles (two above
+// B = 128); inverse: 128-column beta tiles.
+int dwt_split_segments(int direction, const std::vector<int>& group, const std::vector<int>& B,
+                       const std::vector<int>& T, std::vector<unsigned char>& out)
 {
-    std::vector<std::pair<int, SplitItem> > v;
-    const int N = 2 * B, tiles = direction == 0 ? 1 : (N + 127) / 128;
-    for (int c = 0; c < num_classes(B); ++c) {
-        int M, Mp;
-        class_orders(c, M, Mp);
-        for (int t0 = 0; t0 < T; t0 += kTT)
-            for (int tile = 0; tile < tiles; ++tile) {
-                SplitItem it{group, c, t0, T - t0 < kTT ? T - t0 : kTT, tile, 0, 0, 0};
-                v.push_back(std::make_pair(B - M, it));
-            }
+    std::vector<int> order(group.size());
+    for (size_t i = 0; i < order.size(); ++i) order[i] = (int)i;
+    std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return B[a] > B[b]; });
+    std::vector<SplitSeg> segs;
+    int first = 0;
+    for (int i : order) {
+        SplitSeg sg{};
+        sg.group = group[i];
+        sg.first = first;
+        sg.T = T[i];
+        sg.pairs = (T[i] + kNT - 1) / kNT;
+        sg.tiles = direction == 0 ? (B[i] + 127) / 128 : (2 * B[i] + 127) / 128;
+        sg.count = num_classes(B[i]) * sg.pairs * sg.tiles;
+        first += sg.count;
+        segs.push_back(sg);
     }
-    std::stable_sort(v.begin(), v.end(), [](const std::pair<int, SplitItem>& a, const std::pair<int, SplitItem>& b) {
-        return a.first > b.first;
-    });
-    out.resize(v.size() * sizeof(SplitItem));
-    for (size_t i = 0; i < v.size(); ++i) std::memcpy(out.data() + i * sizeof(SplitItem), &v[i].second, sizeof(SplitItem));
-    *n_items = (int)v.size();
+    out.resize(segs.size() * sizeof(SplitSeg));
+    if (!segs.empty()) std::memcpy(out.data(), segs.data(), out.size());
+    return first;
 }
 
+size_t dwt_split_seg_bytes() { return sizeof(SplitSeg); }
+
 int g_split_sms = 0;
+unsigned long long g_split_fail_ns = 0;
 
 cudaError_t dwt_split_prepare()
 {
@@ -722,17 +734,19 @@ cudaError_t dwt_split_prepare()
     return e;
 }
 
-cudaError_t dwt_split_launch(int direction, const DwtGroup* d_groups, const void* d_items, int n_items, int* d_counter,
+void dwt_split_set_fail_ns(unsigned long long ns) { g_split_fail_ns = ns; }
+
+cudaError_t dwt_split_launch(int direction, const DwtGroup* d_groups, const void* d_segs, int nseg, int n_items,
                              int* d_status, cudaStream_t s)
 {
-    if (n_items <= 0) return cudaSuccess;
+    if (n_items <= 0 || nseg <= 0) return cudaSuccess;
     if (g_split_sms <= 0) return cudaErrorNotReady;   // dwt_split_prepare was not called
     const int blocks = n_items < g_split_sms ? n_items : g_split_sms;
-    const SplitItem* it = static_cast<const SplitItem*>(d_items);
+    const SplitSeg* sg = static_cast<const SplitSeg*>(d_segs);
     if (direction == 0)
-        dwt_split_kernel<0><<<blocks, kThreads, kSmemBytes, s>>>(d_groups, it, n_items, d_counter, d_status);
+        dwt_split_kernel<0><<<blocks, kThreads, kSmemBytes, s>>>(d_groups, sg, nseg, n_items, d_status, g_split_fail_ns);
     else
-        dwt_split_kernel<1><<<blocks, kThreads, kSmemBytes, s>>>(d_groups, it, n_items, d_counter, d_status);
+        dwt_split_kernel<1><<<blocks, kThreads, kSmemBytes, s>>>(d_groups, sg, nseg, n_items, d_status, g_split_fail_ns);
     return cudaGetLastError();
 }
 

@@ -4,7 +4,10 @@
 // queue. A scheduler thread forms batches of equal direction and bandwidth (serving.hpp: the
 // arena the HBM budget is counted against, and the batch former), and launches each batch on a
 // free stream as one group: batched FFT passes (gridDim.z = transforms) and one fused DWT launch
-// (dwt_batch.cu) over the batch's (order class, transform block) items. Completion is stamped by
+// (dwt_batch.cu) over the batch's (order class, transform block) items. In split mode
+// (PFSOFT_SERVER_SPLIT) a batch takes requests of one direction and any bandwidths up to 256: FFT
+// passes per bandwidth group, then ONE split-precision DWT launch (dwt_split.cu) over every
+// group's items. Completion is stamped by
 // a host function queued behind the batch on its stream; the scheduler then returns the batch's
 // arena range, frees the stream, and launches whatever waits -- batches of later requests run
 // while earlier ones are still on the device.
@@ -41,6 +44,8 @@ int launch_group(int dir, const BandTables& t, int T, double2** d_grids, double2
                  const DwtItem* d_items, int n_items, int* d_counter, int tpc, double2* const* h_coef,
                  double2* const* h_ws, cudaStream_t s);   // batch.cu
 void group_items(int B, int T, int tpc, std::vector<DwtItem>& out);   // batch.cu
+FftPassArgs group_pass_args(int dir, bool first, const BandTables& t, double2** grids, double2** ws);   // batch.cu
+cudaError_t zero_nyquist_launch(double2** ws, int B, int T, cudaStream_t s);   // batch.cu
 }  // namespace pfsoft_dev
 
 namespace {
@@ -65,9 +70,11 @@ struct Batch;
 
 struct Slot {
     cudaStream_t stream = nullptr;
-    unsigned char* h_stage = nullptr;   // pinned: DwtGroup, then grid / coefficient / spectrum tables
+    unsigned char* h_stage = nullptr;   // pinned: DwtGroup(s), [segments], then grid / coefficient / spectrum tables
     unsigned char* d_stage = nullptr;
     int* d_counter = nullptr;
+    int* h_status = nullptr;            // split mode: mapped host flag a timed-out bounded wait sets
+    int* d_status = nullptr;            // its device alias
     Batch* batch = nullptr;             // the batch on the device, or null
 };
 
@@ -105,6 +112,8 @@ int tpc_for(int B, int k)
 struct pfsoft_server {
     int device = 0;
     int max_batch = 16;
+    bool split = false;          // PFSOFT_SERVER_SPLIT
+    size_t stage_bytes = 0;
     std::vector<Slot> slots;
     void* arena_base = nullptr;
     pfsoft_serving::Arena arena;
@@ -135,6 +144,11 @@ void CUDART_CB on_batch_done(void* p)   // host function: no CUDA calls in here
     Batch* b = static_cast<Batch*>(p);
     b->t_done = now_s();
     pfsoft_server* s = b->srv;
+    int* flag = s->slots[b->slot].h_status;
+    if (flag && *reinterpret_cast<volatile int*>(flag)) {   // the slot's next batch starts after the reap
+        b->status = PFSOFT_ETIMEOUT;
+        *reinterpret_cast<volatile int*>(flag) = 0;
+    }
     {
         std::lock_guard<std::mutex> lk(s->mu);
         s->finished.push_back(b);
@@ -164,9 +178,98 @@ int items_for(pfsoft_server* s, int B, int k, int tpc, const DwtItem** d_items, 
     return PFSOFT_OK;
 }
 
+// Split mode: batch b's requests grouped by bandwidth; FFT passes per group and one
+// split-precision DWT launch over all groups (scheduler thread, mutex not held). Stage layout:
+// DwtGroup[cap], segments[cap], then the grid / coefficient / spectrum pointer tables, members of
+// a group contiguous.
+int launch_split_batch(pfsoft_server* s, Batch* b, const std::vector<Request>& io)
+{
+    Slot& sl = s->slots[b->slot];
+    const int dir = b->plan.dir, k = (int)b->plan.ids.size();
+    const size_t cap = (size_t)s->max_batch;
+    std::map<int, std::vector<int>, std::greater<int> > byB;
+    for (int i = 0; i < k; ++i) byB[b->plan.Bs[i]].push_back(i);
+    const size_t groups_bytes = cap * sizeof(DwtGroup), segs_bytes = cap * dwt_split_seg_bytes();
+    const size_t tab_off = (groups_bytes + segs_bytes + 255) & ~size_t(255);
+    double2** h_tab = reinterpret_cast<double2**>(sl.h_stage + tab_off);
+    double2** d_tab = reinterpret_cast<double2**>(sl.d_stage + tab_off);
+    DwtGroup* h_groups = reinterpret_cast<DwtGroup*>(sl.h_stage);
+    const DwtGroup* d_groups = reinterpret_cast<const DwtGroup*>(sl.d_stage);
+    std::vector<BandTables> tabs;
+    std::vector<int> gidx, gB, gT, gbase;
+    int pos = 0;
+    for (const auto& kv : byB) {
+        BandTables t;
+        const int rc = tables_for(kv.first, sl.stream, &t);
+        if (rc) return rc;
+        const int g = (int)tabs.size();
+        for (size_t m = 0; m < kv.second.size(); ++m) {
+            const Request& r = io[kv.second[m]];
+            const int p = pos + (int)m;
+            h_tab[p] = reinterpret_cast<double2*>(const_cast<double*>(dir == 0 ? r.in : r.out));
+            h_tab[cap + p] = reinterpret_cast<double2*>(const_cast<double*>(dir == 0 ? r.out : r.in));
+            h_tab[2 * cap + p] = reinterpret_cast<double2*>(static_cast<char*>(s->arena_base) + b->plan.offset +
+                                                              b->plan.offs[kv.second[m]]);
+        }
+        DwtGroup d;
+        d.B = t.B;
+        d.N = t.N;
+        d.T = (int)kv.second.size();
+        d.cosb = t.cosb;
+        d.w = t.w;
+        d.normf = t.normf;
+        d.pw_sin = t.pw_sin;
+        d.pw_cos = t.pw_cos;
+        d.rc_cf = t.rc_cf;
+        d.rc_f1 = t.rc_f1;
+        d.X = d_tab + 2 * cap + pos;
+        d.coeffs = d_tab + cap + pos;
+        h_groups[g] = d;
+        tabs.push_back(t);
+        gidx.push_back(g);
+        gB.push_back(t.B);
+        gT.push_back(d.T);
+        gbase.push_back(pos);
+        pos += d.T;
+    }
+    std::vector<unsigned char> segs;
+    const int n_items = dwt_split_segments(dir, gidx, gB, gT, segs);
+    std::memcpy(sl.h_stage + groups_bytes, segs.data(), segs.size());
+    cudaError_t e = cudaSuccess;
+    for (int i = 0; i < k && e == cudaSuccess; ++i)
+        if (io[i].ready) e = cudaStreamWaitEvent(sl.stream, io[i].ready, 0);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(sl.d_stage, sl.h_stage, s->stage_bytes, cudaMemcpyHostToDevice, sl.stream);
+    const int sign = dir == 0 ? -1 : +1;
+    auto fft = [&](size_t g, bool first) {
+        const FftPassArgs a = group_pass_args(dir, first, tabs[g], d_tab + gbase[g], d_tab + 2 * cap + gbase[g]);
+        return fft_pass_launch(nullptr, nullptr, a, tabs[g].N, sign, sl.stream, gT[g]);
+    };
+    for (size_t g = 0; g < tabs.size() && e == cudaSuccess; ++g) {
+        double2** ws = d_tab + 2 * cap + gbase[g];
+        double2** cf = d_tab + cap + gbase[g];
+        if (dir == 0) {
+            e = fft(g, true);
+            if (e == cudaSuccess) e = fft(g, false);
+        } else {
+            e = zero_nyquist_launch(ws, gB[g], gT[g], sl.stream);
+        }
+        if (e == cudaSuccess) e = dwt_split_scales(dir, gB[g], gT[g], ws, cf, tabs[g].w, sl.stream);
+    }
+    if (e == cudaSuccess)
+        e = dwt_split_launch(dir, d_groups, sl.d_stage + groups_bytes, (int)tabs.size(), n_items, sl.d_status, sl.stream);
+    for (size_t g = 0; dir == 1 && g < tabs.size() && e == cudaSuccess; ++g) {
+        e = fft(g, true);
+        if (e == cudaSuccess) e = fft(g, false);
+    }
+    if (e == cudaSuccess) e = cudaLaunchHostFunc(sl.stream, on_batch_done, b);
+    if (e != cudaSuccess) return fail(PFSOFT_ECUDA, std::string("server split batch: ") + cudaGetErrorString(e));
+    return PFSOFT_OK;
+}
+
 // Launches batch b on its slot (scheduler thread, mutex not held).
 int launch_batch(pfsoft_server* s, Batch* b, const std::vector<Request>& io)
 {
+    if (s->split) return launch_split_batch(s, b, io);
     Slot& sl = s->slots[b->slot];
     const int B = b->plan.B, k = (int)b->plan.ids.size(), dir = b->plan.dir;
     BandTables t;
@@ -190,7 +293,7 @@ int launch_batch(pfsoft_server* s, Batch* b, const std::vector<Request>& io)
         double* out = io[i].out;
         h_grid[i] = reinterpret_cast<double2*>(const_cast<double*>(dir == 0 ? in : out));
         h_coef[i] = reinterpret_cast<double2*>(const_cast<double*>(dir == 0 ? out : in));
-        h_ws[i] = reinterpret_cast<double2*>(static_cast<char*>(s->arena_base) + b->plan.offset + (size_t)i * b->plan.stride);
+        h_ws[i] = reinterpret_cast<double2*>(static_cast<char*>(s->arena_base) + b->plan.offset + b->plan.offs[i]);
     }
     DwtGroup g;
     g.B = B;
@@ -337,25 +440,42 @@ extern "C" {
 
 int pfsoft_server_create(size_t budget_bytes, int max_batch, int streams, pfsoft_server** out)
 {
+    return pfsoft_server_create_ex(budget_bytes, max_batch, streams, 0, out);
+}
+
+int pfsoft_server_create_ex(size_t budget_bytes, int max_batch, int streams, int flags, pfsoft_server** out)
+{
     set_last_error("");
     if (!out) return fail(PFSOFT_EINVAL, "null output handle");
     *out = nullptr;
     if (max_batch < 1 || max_batch > kMaxBatchLimit) return fail(PFSOFT_EINVAL, "max_batch must be in [1, 256]");
     if (streams < 1 || streams > kMaxStreams) return fail(PFSOFT_EINVAL, "streams must be in [1, 16]");
+    if (flags & ~PFSOFT_SERVER_SPLIT) return fail(PFSOFT_EINVAL, "unknown server flag");
     if (budget_bytes < pfsoft_workspace_bytes(1)) return fail(PFSOFT_EINVAL, "budget below one transform");
     pfsoft_server* s = new pfsoft_server();
     s->max_batch = max_batch;
+    s->split = (flags & PFSOFT_SERVER_SPLIT) != 0;
     s->sched.set_max_batch(max_batch);
+    s->sched.set_mixed(s->split);
     cudaError_t e = cudaGetDevice(&s->device);
+    if (e == cudaSuccess && s->split) e = dwt_split_prepare();
     if (e == cudaSuccess) e = cudaMalloc(&s->arena_base, budget_bytes);
     s->arena.reset(e == cudaSuccess ? budget_bytes : 0, 256);
     s->slots.resize(streams);
-    const size_t stage = kStageHeader + 3 * (size_t)max_batch * sizeof(double2*);
+    const size_t tables = 3 * (size_t)max_batch * sizeof(double2*);
+    const size_t stage = s->split ? (((size_t)max_batch * (sizeof(DwtGroup) + dwt_split_seg_bytes()) + 255) & ~size_t(255)) + tables
+                                  : kStageHeader + tables;
+    s->stage_bytes = stage;
     for (auto& sl : s->slots) {
         if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&sl.stream, cudaStreamNonBlocking);
         if (e == cudaSuccess) e = cudaHostAlloc(reinterpret_cast<void**>(&sl.h_stage), stage, cudaHostAllocDefault);
         if (e == cudaSuccess) e = cudaMalloc(reinterpret_cast<void**>(&sl.d_stage), stage);
         if (e == cudaSuccess) e = cudaMalloc(reinterpret_cast<void**>(&sl.d_counter), sizeof(int));
+        if (e == cudaSuccess && s->split) e = cudaHostAlloc(reinterpret_cast<void**>(&sl.h_status), sizeof(int), cudaHostAllocMapped);
+        if (e == cudaSuccess && s->split) {
+            *sl.h_status = 0;
+            e = cudaHostGetDevicePointer(reinterpret_cast<void**>(&sl.d_status), sl.h_status, 0);
+        }
         if (e == cudaSuccess) std::memset(sl.h_stage, 0, stage);
     }
     if (e != cudaSuccess) {
@@ -366,6 +486,7 @@ int pfsoft_server_create(size_t budget_bytes, int max_batch, int streams, pfsoft
             cudaFreeHost(sl.h_stage);
             cudaFree(sl.d_stage);
             cudaFree(sl.d_counter);
+            cudaFreeHost(sl.h_status);
         }
         cudaFree(s->arena_base);
         delete s;
@@ -392,6 +513,7 @@ int pfsoft_server_destroy(pfsoft_server* s)
         cudaFreeHost(sl.h_stage);
         cudaFree(sl.d_stage);
         cudaFree(sl.d_counter);
+        cudaFreeHost(sl.h_status);
     }
     for (auto& kv : s->items) cudaFree(kv.second.first);
     for (cudaEvent_t ev : s->dead_events)
@@ -408,10 +530,11 @@ int pfsoft_server_submit(pfsoft_server* s, int direction, int B, const double* d
     *id = 0;
     if (direction != 0 && direction != 1) return fail(PFSOFT_EINVAL, "direction must be 0 (DSOFT) or 1 (iDSOFT)");
     if (B < 1 || B > 512) return fail(PFSOFT_EINVAL, "bandwidth must be in [1, 512]");
+    if (s->split && !dwt_split_supported(B)) return fail(PFSOFT_EINVAL, "a split-mode server takes bandwidths up to 256");
     if (!d_in || !d_out) return fail(PFSOFT_EINVAL, "null buffer");
     if ((reinterpret_cast<uintptr_t>(d_in) & 15) || (reinterpret_cast<uintptr_t>(d_out) & 15))
         return fail(PFSOFT_EINVAL, "buffers must be 16-byte aligned");
-    const size_t bytes = pfsoft_workspace_bytes(B);
+    const size_t bytes = pfsoft_workspace_bytes(B) + (s->split ? dwt_split_aux_elems(B) * sizeof(double2) : 0);
     {
         std::lock_guard<std::mutex> lk(s->mu);
         if (s->stop) return fail(PFSOFT_EBUSY, "server is shutting down");

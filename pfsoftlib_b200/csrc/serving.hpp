@@ -4,8 +4,8 @@
 //
 // A request needs, besides its caller-owned input and output, one beta-innermost spectrum of
 // (2B)^3 complex doubles on the device while it runs. The server reserves one arena of the HBM
-// budget at start-up; a batch of k equal-bandwidth requests takes one contiguous k-spectrum range
-// of it and gives it back when the batch finishes. A request is admitted to the GPU when its
+// budget at start-up; a batch of k requests takes one contiguous range of it (the sum of their
+// workspaces) and gives it back when the batch finishes. A request is admitted to the GPU when its
 // batch fits; until then it waits in the queue.
 #pragma once
 
@@ -106,17 +106,19 @@ struct Pending {
 };
 
 struct BatchPlan {
-    int dir = 0, B = 0;
+    int dir = 0, B = 0;           // B: the bandwidth of the first request (all of them unless mixed)
     std::vector<long long> ids;   // FIFO order
-    long long offset = -1;        // arena range of ids.size() workspaces, each `stride` bytes
-    size_t stride = 0;
+    std::vector<int> Bs;          // bandwidth of each request
+    std::vector<size_t> offs;     // workspace of each request, relative to `offset`
+    long long offset = -1;        // arena range of the batch
+    size_t stride = 0;            // workspace bytes of one request when all bandwidths are equal
 };
 
 // FIFO queue with batch forming: the next batch takes the oldest waiting request and up to
-// max_batch - 1 later requests of the same direction and bandwidth, as many as the arena can
-// hold. When even one of them does not fit, younger groups may go ahead (backfill), unless the
-// oldest request has waited longer than `aging` seconds, in which case nothing else starts until
-// memory frees up for it.
+// max_batch - 1 later requests of the same direction and bandwidth (with mixed bandwidths on: of
+// the same direction, any bandwidth), as many as the arena can hold. When even one of them does
+// not fit, younger groups may go ahead (backfill), unless the oldest request has waited longer
+// than `aging` seconds, in which case nothing else starts until memory frees up for it.
 class Scheduler {
   public:
     Scheduler(int max_batch = 16, double aging = 0.05) : max_batch_(std::max(1, max_batch)), aging_(aging) {}
@@ -124,6 +126,8 @@ class Scheduler {
     void set_max_batch(int m) { max_batch_ = std::max(1, m); }
     int max_batch() const { return max_batch_; }
     void set_aging(double s) { aging_ = s; }
+    void set_mixed(bool on) { mixed_ = on; }
+    bool mixed() const { return mixed_; }
 
     void push(const Pending& p) { q_.push_back(p); }
     size_t pending() const { return q_.size(); }
@@ -155,22 +159,30 @@ class Scheduler {
         bool first = true;
         for (size_t i = 0; i < q_.size(); ++i) {
             const Pending& head = q_[i];
-            const std::pair<int, int> key(head.dir, head.B);
+            const std::pair<int, int> key(head.dir, mixed_ ? 0 : head.B);
             if (std::find(tried.begin(), tried.end(), key) != tried.end()) continue;
             tried.push_back(key);
             std::vector<size_t> members;
             for (size_t j = i; j < q_.size() && (int)members.size() < max_batch_; ++j)
-                if (q_[j].dir == head.dir && q_[j].B == head.B) members.push_back(j);
-            const size_t stride = arena.footprint(head.bytes);
+                if (q_[j].dir == head.dir && (mixed_ || q_[j].B == head.B)) members.push_back(j);
+            // prefix sums of the members' footprints: the first k members take sum[k] bytes
+            std::vector<size_t> sum(members.size() + 1, 0);
+            for (size_t m = 0; m < members.size(); ++m) sum[m + 1] = sum[m] + arena.footprint(q_[members[m]].bytes);
             for (size_t k = members.size(); k >= 1; --k) {
-                const long long off = arena.alloc(stride * k);
+                const long long off = arena.alloc(sum[k]);
                 if (off < 0) continue;
                 out->dir = head.dir;
                 out->B = head.B;
                 out->offset = off;
-                out->stride = stride;
+                out->stride = arena.footprint(head.bytes);
                 out->ids.clear();
-                for (size_t m = 0; m < k; ++m) out->ids.push_back(q_[members[m]].id);
+                out->Bs.clear();
+                out->offs.clear();
+                for (size_t m = 0; m < k; ++m) {
+                    out->ids.push_back(q_[members[m]].id);
+                    out->Bs.push_back(q_[members[m]].B);
+                    out->offs.push_back(sum[m]);
+                }
                 for (size_t m = k; m-- > 0;) q_.erase(q_.begin() + (long)members[m]);
                 return true;
             }
@@ -183,6 +195,7 @@ class Scheduler {
   private:
     int max_batch_;
     double aging_;
+    bool mixed_ = false;
     std::deque<Pending> q_;
 };
 

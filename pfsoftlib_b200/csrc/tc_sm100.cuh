@@ -1,10 +1,11 @@
-// Thin wrappers over the sm_100a tensor-core instructions used by the split-precision DWT
-// (tcgen05.* with operands in shared memory and the accumulator in tensor memory), and the
-// mbarrier operations that order them. Inline PTX, one instruction per function.
+// Thin wrappers over the sm_100a instructions used by the split-precision DWT: tcgen05.* with
+// operands in shared memory and the accumulator in tensor memory, the mbarrier operations that
+// order them, and the async-proxy fences. Inline PTX, one instruction per function.
 //
-// Shared-memory operand layout (no swizzle): the tensor core reads 8 x 16-byte "core matrices".
-//   K-major   element (row r, k) at  (k/8)*LBO + (r/8)*SBO + (r%8)*16 + (k%8)*2
-//   MN-major  element (mn m, k)  at  (m/8)*SBO + (k/8)*LBO + (k%8)*16 + (m%8)*2
+// Shared-memory operand layouts (no swizzle, 8-bit elements): the tensor core reads "core
+// matrices" of 8 rows x 16 bytes, each 128 contiguous bytes.
+//   K-major   element (row r, k) at  (r/8)*SBO + (k/16)*LBO + (r%8)*16 + (k%16)
+//   MN-major  element (mn m, k)  at  (m/16)*SBO + (k/8)*LBO + (k%8)*16 + (m%16)
 // Tensor-memory addresses: bits 31..16 lane, bits 15..0 column (32-bit cells).
 #pragma once
 
@@ -28,12 +29,12 @@ __device__ __forceinline__ uint64_t sdesc(uint32_t smem_addr, uint32_t lbo_bytes
     return d;                 // base offset 0, lbo mode 0, layout SWIZZLE_NONE (0)
 }
 
-// ---- instruction descriptor: kind::f16 with BF16 A/B, F32 accumulator -----------------------
-__host__ __device__ constexpr uint32_t idesc_bf16(int M, int N, bool a_mn_major, bool b_mn_major)
+// ---- instruction descriptor: kind::i8 with signed 8-bit A/B, S32 accumulator ----------------
+__host__ __device__ constexpr uint32_t idesc_s8(int M, int N, bool a_mn_major, bool b_mn_major)
 {
-    return (1u << 4)                          // D format F32
-         | (1u << 7)                          // A format BF16
-         | (1u << 10)                         // B format BF16
+    return (2u << 4)                          // D format S32
+         | (1u << 7)                          // A format signed 8-bit
+         | (1u << 10)                         // B format signed 8-bit
          | ((a_mn_major ? 1u : 0u) << 15)
          | ((b_mn_major ? 1u : 0u) << 16)
          | ((uint32_t)(N >> 3) << 17)
@@ -56,13 +57,13 @@ __device__ __forceinline__ void tmem_dealloc(uint32_t taddr, uint32_t ncols)
     asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(taddr), "r"(ncols) : "memory");
 }
 
-// ---- MMA: D[tmem] (+)= A[smem] * B[smem] -------------------------------------------------------
-__device__ __forceinline__ void mma_bf16(uint32_t d_tmem, uint64_t a_desc, uint64_t b_desc, uint32_t idesc, bool accumulate)
+// ---- MMA: D[tmem] (+)= A[smem] * B[smem], signed 8-bit operands, exact S32 accumulation ---------
+__device__ __forceinline__ void mma_s8(uint32_t d_tmem, uint64_t a_desc, uint64_t b_desc, uint32_t idesc, bool accumulate)
 {
     asm volatile(
         "{\n\t.reg .pred p;\n\t"
         "setp.ne.b32 p, %4, 0;\n\t"
-        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}"
+        "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, p;\n\t}"
         ::"r"(d_tmem), "l"(a_desc), "l"(b_desc), "r"(idesc), "r"(accumulate ? 1u : 0u)
         : "memory");
 }
@@ -80,8 +81,8 @@ __device__ __forceinline__ void fence_after_sync() { asm volatile("tcgen05.fence
 // Generic-proxy shared-memory writes become visible to the tensor core (async proxy).
 __device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
 
-// ---- tensor memory -> registers: 32 lanes x 32-bit, x16 / x32 consecutive columns --------------
-__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&v)[16])
+// ---- tensor memory -> registers: 32 lanes x 32-bit, 16 consecutive columns ---------------------
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, int32_t (&v)[16])
 {
     uint32_t r[16];
     asm volatile(
@@ -91,7 +92,7 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&v)[16])
         : "r"(taddr)
         : "memory");
 #pragma unroll
-    for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
+    for (int i = 0; i < 16; ++i) v[i] = (int32_t)r[i];
 }
 __device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
 
@@ -101,6 +102,11 @@ __device__ __forceinline__ void mbar_init(uint64_t* mbar, uint32_t count)
     asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(mbar)), "r"(count) : "memory");
 }
 __device__ __forceinline__ void mbar_fence_init() { asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory"); }
+
+__device__ __forceinline__ void mbar_arrive(uint64_t* mbar)
+{
+    asm volatile("{\n\t.reg .b64 st;\n\tmbarrier.arrive.shared::cta.b64 st, [%0];\n\t}" ::"r"(smem_u32(mbar)) : "memory");
+}
 
 __device__ __forceinline__ bool mbar_try_wait(uint64_t* mbar, uint32_t parity)
 {
@@ -115,22 +121,36 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* mbar, uint32_t parity)
     return ok != 0;
 }
 
-// Waits for the phase with the given parity to complete; gives up after about `limit_ns`
-// nanoseconds and returns false (the caller records the failure and leaves).
 __device__ __forceinline__ uint64_t globaltimer_ns()
 {
     uint64_t t;
     asm volatile("mov.u64 %0, %globaltimer;" : "=l"(t));
     return t;
 }
-__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* mbar, uint32_t parity, uint64_t limit_ns)
+
+// Waits for the phase with the given parity to complete. Gives up after about `limit_ns`
+// nanoseconds, or as soon as *abort is set by another thread of the CTA; on giving up it sets
+// *abort and returns false (the caller leaves its loop).
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* mbar, uint32_t parity, uint64_t limit_ns, volatile int* abort)
 {
     if (mbar_try_wait(mbar, parity)) return true;
     const uint64_t t0 = globaltimer_ns();
     for (;;) {
         if (mbar_try_wait(mbar, parity)) return true;
-        if (globaltimer_ns() - t0 > limit_ns) return false;
+        if (*abort) return false;
+        if (globaltimer_ns() - t0 > limit_ns) {
+            *abort = 1;
+            return false;
+        }
     }
+}
+
+// ---- byte shuffles for digit planes ----------------------------------------------------------
+__device__ __forceinline__ uint32_t prmt(uint32_t a, uint32_t b, uint32_t sel)
+{
+    uint32_t d;
+    asm("prmt.b32 %0, %1, %2, %3;" : "=r"(d) : "r"(a), "r"(b), "r"(sel));
+    return d;
 }
 
 }  // namespace tc

@@ -10,7 +10,10 @@ such call becomes a request against a server that keeps the data on the device:
 
 Requests of equal direction and bandwidth that wait together run as one batch; a batch starts as
 soon as a stream and room in the workspace arena (the HBM budget) are free, while earlier
-batches are still on the device. A request keeps references to its tensors until it finishes.
+batches are still on the device. With ``split=True`` a batch takes waiting requests of one
+direction and any bandwidths up to 256 and runs their Wigner transforms in one split-precision
+tensor-core launch (``PFSOFT_SERVER_SPLIT``). A request keeps references to its tensors until it
+finishes.
 """
 from __future__ import annotations
 
@@ -19,6 +22,7 @@ import ctypes
 from . import _lib
 
 DSOFT, IDSOFT = 0, 1
+SERVER_SPLIT = 1
 
 
 class ServerStats(ctypes.Structure):
@@ -82,11 +86,14 @@ class Request:
 
 
 class TransformServer:
-    def __init__(self, budget_bytes: int = 160 << 30, max_batch: int = 16, streams: int = 4):
+    def __init__(self, budget_bytes: int = 160 << 30, max_batch: int = 16, streams: int = 4, split: bool = False):
         self._lib = _lib.load()
+        self._h = None
         h = ctypes.c_void_p()
-        _lib.check(self._lib.pfsoft_server_create(int(budget_bytes), int(max_batch), int(streams), ctypes.byref(h)))
+        _lib.check(self._lib.pfsoft_server_create_ex(int(budget_bytes), int(max_batch), int(streams),
+                                                     SERVER_SPLIT if split else 0, ctypes.byref(h)))
         self._h = h
+        self.split = bool(split)
 
     # -- requests --------------------------------------------------------------------------
     def submit(self, direction: int, B: int, inp, out, stream=None) -> Request:

@@ -88,6 +88,35 @@ static void admission_and_backfill()
     CHECK(s.pending() == 1);
 }
 
+// Mixed bandwidths (split mode): a batch takes requests of one direction and any bandwidths, each
+// with its own workspace size at its own offset inside the batch's range.
+static void mixed_batches()
+{
+    Arena a(10000, 1);
+    Scheduler s(3, 1.0);
+    s.set_mixed(true);
+    s.push(req(1, 0, 16, 1000, 0));
+    s.push(req(2, 1, 20, 1500, 0));
+    s.push(req(3, 0, 32, 2000, 0));
+    s.push(req(4, 0, 17, 500, 0));
+    s.push(req(5, 0, 16, 1000, 0));
+    BatchPlan p;
+    CHECK(s.next(a, 0, &p));   // direction 0, oldest three: 1, 3, 4
+    CHECK(p.dir == 0 && p.ids == std::vector<long long>({1, 3, 4}));
+    CHECK(p.Bs == std::vector<int>({16, 32, 17}));
+    CHECK(p.offs == std::vector<size_t>({0, 1000, 3000}) && p.offset == 0 && a.used() == 3500);
+    CHECK(s.next(a, 0, &p) && p.dir == 1 && p.ids == std::vector<long long>({2}) && p.offset == 3500);
+    // room for 5000 more: request 5 alone
+    CHECK(s.next(a, 0, &p) && p.ids == std::vector<long long>({5}) && p.offs == std::vector<size_t>({0}));
+    CHECK(s.empty());
+    // a batch that does not fit whole shrinks to the prefix that does
+    Arena b(2550, 1);
+    s.push(req(6, 0, 16, 1000, 0));
+    s.push(req(7, 0, 64, 1500, 0));
+    s.push(req(8, 0, 8, 100, 0));
+    CHECK(s.next(b, 0, &p) && p.ids == std::vector<long long>({6, 7}) && b.used() == 2500);
+}
+
 static void cancel_and_shutdown()
 {
     Scheduler s(8, 1.0);
@@ -170,6 +199,7 @@ int main()
 {
     arena_basics();
     batching();
+    mixed_batches();
     admission_and_backfill();
     cancel_and_shutdown();
     quantiles();

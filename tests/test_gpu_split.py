@@ -1,5 +1,6 @@
-"""Split-precision DWT (PFSOFT_BATCH_SPLIT): tensor-core digit products against the FP64 path,
-the compiled reference's golden vectors, and mixed plans where some bandwidths stay on FP64.
+"""Split-precision DWT (PFSOFT_BATCH_SPLIT): exact 8-bit digit products on the tensor cores
+against the FP64 path, the compiled reference's golden vectors, the oracle, mixed plans of
+uneven bandwidths, and the kernel's bounded-wait exit.
 
 Tolerance: relative L2 error <= 1e-11 against FP64 results (the engine's stated bound for the
 split path; the digit arithmetic itself gives about 1e-13)."""
@@ -51,10 +52,11 @@ def _coeffs(lib, bws, seed0=300, kind=1, power=1.0):
 
 
 def test_supported_bandwidths(lib):
-    assert [B for B in range(1, 300) if lib.pfsoft_split_supported(B)] == list(range(16, 129, 16))
+    assert [B for B in range(0, 300) if lib.pfsoft_split_supported(B)] == list(range(1, 257))
 
 
-@pytest.mark.parametrize("B,T", [(16, 1), (16, 4), (32, 6), (64, 4), (128, 5)])
+@pytest.mark.parametrize("B,T", [(1, 1), (3, 2), (16, 1), (16, 4), (32, 6), (37, 3), (64, 4), (100, 2), (128, 5),
+                                 (192, 2), (256, 2)])
 def test_split_matches_fp64(lib, B, T):
     bws = [B] * T
     cs = _coeffs(lib, bws, seed0=1000 * B + T)
@@ -94,9 +96,53 @@ def test_split_against_reference_golden(lib, golden):
         assert _rel(outs[t], fref) <= REL_TOL
 
 
+def test_split_against_oracle(lib, oracle):
+    """B = 20 and 33 (odd sizes, partial chunks and tiles): split-path grids and coefficients
+    against the long-double oracle's IDSOFT / DSOFT of the same inputs."""
+    import torch
+    from oracle import oracle as orc
+    for B in (20, 33):
+        c = orc.coeffs_uniform(B, seed=B)
+        dc = torch.from_numpy(c).to("cuda")
+        grids, back = _run(lib, [B, B], [dc.clone(), dc.clone()], SPLIT)
+        g_ref = oracle.idsoft(c, B)
+        f_ref = oracle.dsoft(grids[0].cpu().numpy())
+        for t in range(2):
+            assert orc.rel_l2(grids[t].cpu().numpy(), g_ref) <= REL_TOL, f"B={B} grid"
+        assert orc.rel_l2(back[0].cpu().numpy(), f_ref) <= REL_TOL, f"B={B} coefficients"
+
+
+def test_bounded_wait_exit(lib):
+    """A split launch whose first wait (before any MMA) runs out leaves cleanly: the plan's status
+    reads PFSOFT_ETIMEOUT, the context stays usable, and a new plan then runs clean."""
+    import torch
+    bws = [16, 16]
+    cs = _coeffs(lib, bws, seed0=5)
+    s = torch.cuda.current_stream().cuda_stream
+    grids = [torch.empty((32,) * 3, dtype=torch.complex128, device="cuda") for _ in bws]
+    plan = ctypes.c_void_p()
+    assert lib.pfsoft_batch_create((ctypes.c_int * 2)(*bws), 2, 0, SPLIT | 1, ctypes.byref(plan)) == 0
+    cp = (ctypes.c_void_p * 2)(*[t.data_ptr() for t in cs])
+    gp = (ctypes.c_void_p * 2)(*[t.data_ptr() for t in grids])
+    try:
+        assert lib.pfsoft_test_split_wait_ns(1_000_000) == 0      # 1 ms
+        assert lib.pfsoft_batch_idsoft(plan, cp, gp, s) == 0
+        torch.cuda.synchronize()
+    finally:
+        lib.pfsoft_test_split_wait_ns(0)
+    assert lib.pfsoft_batch_status(plan) == 3                       # PFSOFT_ETIMEOUT
+    lib.pfsoft_batch_destroy(plan)
+    g64, c64 = _run(lib, bws, cs, 0)
+    gsp, csp = _run(lib, bws, cs, SPLIT)
+    for t in range(2):
+        assert _rel(gsp[t], g64[t]) <= REL_TOL
+        assert _rel(csp[t], c64[t]) <= REL_TOL
+
+
 def test_mixed_plan_split_and_fp64(lib):
-    """Bandwidths the split kernel takes (16, 32, 64) and ones it leaves to FP64 (24, 40) in one plan."""
-    bws = [16, 24, 32, 32, 40, 64, 64, 64, 64, 16]
+    """Uneven bandwidths in one split plan, every group in the one split launch, against the FP64
+    plan (which runs B <= 128 fused and larger ones per transform)."""
+    bws = [16, 24, 32, 32, 40, 64, 64, 64, 64, 16, 97, 130, 130]
     cs = _coeffs(lib, bws, seed0=77, kind=2, power=1.5)
     g64, c64 = _run(lib, bws, cs, 0)
     gsp, csp = _run(lib, bws, cs, SPLIT)
