@@ -1,16 +1,25 @@
 """Benchmark: DSOFT + iDSOFT transforms/s at bandwidth B = 128 (one B200 per rank).
 
 One step = one iDSOFT (2,796,160 coefficients -> 256^3 complex128 grid) followed by one DSOFT
-of that grid (the single-transform workload at B = 128), i.e. 2 transforms per step. Inputs are
-seeded synthetic coefficients: uniform phase, magnitude (1+l)^-1 |N(0,1)|, PCG64 seed 1.
+of that grid (the single-transform workload at B = 128), i.e. 2 transforms per step, on the FP64
+drop-in path. Inputs are seeded synthetic coefficients: uniform phase, magnitude
+(1+l)^-1 |N(0,1)|, PCG64 seed 1.
 
   value     transforms/s with everything resident in HBM, device time (CUDA events) over the
             K timed steps, max over ranks; every buffer (268 MB grid) exceeds the 126 MB L2.
   e2e       the same metric through the host-facing C ABI (pfsoft_idsoft_host /
-            pfsoft_dsoft_host) from pinned host memory, copies inside the timed region.
+            pfsoft_dsoft_host) from pinned host memory, copies inside the timed region;
+            e2e_pageable the same from pageable memory (what the C++ drop-in header hands over).
   roofline  the dominant stage, timed with CUDA events per stage inside the timed region.
   cpu_baseline  the reference's own CPU DSOFT/IDSOFT (compiled from its sources with a project
             FFT in FFTW's place) on a bounded sample, rank 0 at N = 1 only.
+At N = 1 the line also carries the other workloads in compact form (skip with --no-extras):
+  mixed     256 transforms of uneven bandwidth: plain FP64 loop, FP64 batch, split-precision
+            batch, split-precision server (saturated), with errors against FP64 and the oracle.
+  b256      8 transforms at B = 256: FP64 batch against the split-precision batch, errors against
+            FP64 and the reference CPU DSOFT.
+  serving   Poisson arrivals, bandwidths log-uniform over the integers 16..256: p50 / p99 latency
+            and transforms/s of the split-precision server and of the plain per-request FP64 path.
 
 --impl reference times the reference CPU implementation alone on the host cores.
 Multi-GPU (torchrun): every rank runs its own transforms (independent replicas, weak scaling);
@@ -47,7 +56,7 @@ FFT_PASS_BYTES = 2 * GRID_BYTES
 DWT_FLOPS = 8 * B * B * (4 * B * B - 1) / 3
 
 
-def workload_config(l2_note: str) -> dict:
+def workload_config() -> dict:
     return {
         "workload": "single transform at B=128: iDSOFT of 2,796,160 complex128 coefficients to a "
                     "256^3 complex128 grid, then DSOFT of that grid",
@@ -56,8 +65,19 @@ def workload_config(l2_note: str) -> dict:
         "coefficients": COEF_COUNT,
         "transforms_per_step": TRANSFORMS_PER_STEP,
         "inputs": "seeded synthetic (PCG64 seed 1): uniform phase, |f| = (1+l)^-1 |N(0,1)|",
-        "l2": l2_note,
+        "l2": "inputs larger than L2: 268 MB grid and workspace, 45 MB coefficients",
     }
+
+
+def measured_peaks() -> dict:
+    """HBM copy bandwidth of this pool's B200s from MEASURED_PEAKS.json (written next to this
+    file by the machine's operators), else the pool's earlier fallback figure."""
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            d = json.load(f)
+        return {"hbm_gbs": float(d["hbm_gbs"]), "source": "measured (MEASURED_PEAKS.json hbm_gbs)"}
+    except (OSError, ValueError, KeyError, TypeError):
+        return {"hbm_gbs": 6650.0, "source": "fallback 6.65 TB/s (MEASURED_PEAKS.json absent)"}
 
 
 def parse():
@@ -74,8 +94,9 @@ def parse():
                          "the ranks (strong scaling)")
     ap.add_argument("--rates", default="50,100,200,500,1000,2000", help="serve: offered requests/s")
     ap.add_argument("--seconds", type=float, default=5.2,
-                    help="serve: arrival window per rate (5.2 s over the default rates: ~20,000 requests)")
+                    help="serve: arrival window per rate (5.2 s over the default rates: ~20,000 requests per arm)")
     ap.add_argument("--budget-gb", type=float, default=160.0, help="serve: HBM budget of the server's arena")
+    ap.add_argument("--no-extras", action="store_true", help="single: skip the mixed / b256 / serving sections")
     return ap.parse_args()
 
 
@@ -163,15 +184,15 @@ def cpu_reference_sample(steps: int, warmup: int, coeffs) -> dict:
     else:
         ora = orc.Oracle()
         kind = "port"
-        threads = os.cpu_count() or 1
+        threads = 1
         t0 = time.perf_counter()
         g = ora.idsoft(coeffs, B)
         ora.dsoft(g)
         t = time.perf_counter() - t0
         steps = 1
-        sample = "1 x (IDSOFT + DSOFT) at B=128 through the long-double C restatement (oracle/)"
+        sample = "1 x (IDSOFT + DSOFT) at B=128 through the long-double C restatement (oracle/), one thread"
     return {"value": TRANSFORMS_PER_STEP * steps / t, "unit": UNIT, "cores": threads, "kind": kind,
-            "sample": sample, "seconds": t}
+            "sample": sample, "seconds": t, "steps": steps}
 
 
 def run_reference_arm(args):
@@ -181,278 +202,432 @@ def run_reference_arm(args):
     from oracle import oracle as orc
 
     coeffs = orc.coeffs_decaying(B, seed=1, power=1.0, normal_mag=True)
-    steps = max(1, min(args.steps, 20))
-    warm = 1 if args.warmup > 0 else 0
+    # each step is one IDSOFT + DSOFT at B = 128 (~0.65 s on 16 cores): at most 100 steps and
+    # 10 warm-up steps keep the arm within a few minutes
+    steps = max(1, min(args.steps, 100))
+    warm = max(0, min(args.warmup, 10))
     cb = cpu_reference_sample(steps, warm, coeffs)
     line = {
         "impl": "reference", "metric": METRIC, "value": cb["value"], "unit": UNIT, "n_gpus": args.gpus,
-        "steps": steps, "warmup": warm, "ms_per_step": 1e3 * cb["seconds"] / steps, "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f64 (long double DWT accumulation)", "data": "synthetic",
-        "config": workload_config("host memory"),
+        "steps": cb["steps"], "warmup": warm, "ms_per_step": 1e3 * cb["seconds"] / cb["steps"], "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": workload_config(),
         "cpu_baseline": {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")},
         "e2e": {"value": cb["value"], "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "note": "the reference's DWT accumulates in long double (x87); its FFT slot holds the project FFT",
     }
     print(json.dumps(line), flush=True)
 
 
-# ----------------------------------------------------------------------------- GPU arm
+# ----------------------------------------------------------------------------- GPU workloads
 
 MIXED_BANDS = (32, 48, 64, 96, 128)
+SPLIT, NO_GRAPH = 2, 1
 
 
-def run_served(lib, bws, coeffs, grids, plain_back, ms_plain, seed=3):
-    """The mixed workload as requests to the transform server (pfsoft_server_*): 256 iDSOFT
-    requests (coefficients -> fresh grids) and 256 DSOFT requests (the plain loop's grids ->
-    fresh coefficients), independent, submitted in a shuffled order.
-      saturated  all 512 submitted at once; transforms/s = 512 / (first submit -> last result)
-      open_loop  Poisson arrivals at 60% of the saturated rate; p50 / p99 submit -> result
-    Results are checked against the plain loop's (same kernels: equal)."""
+def _dev_coeffs(lib, B, seed, kind, power, s):
+    import torch
+    c = torch.empty(B * (4 * B * B - 1) // 3, dtype=torch.complex128, device="cuda")
+    assert lib.pfsoft_cuda_random_coeffs(c.data_ptr(), B, int(seed), kind, float(power), s) == 0
+    return c
+
+
+def _rel(a, b) -> float:
+    import torch
+    return (torch.linalg.vector_norm(a - b) / torch.linalg.vector_norm(b)).item()
+
+
+def _timed(fn, steps, warmup):
+    """Device milliseconds per call of fn (CUDA events on torch's current stream)."""
+    import torch
+    for _ in range(max(1, warmup)):
+        fn()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(steps):
+        fn()
+    e1.record()
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1) / steps
+
+
+class _Plan:
+    """A batch plan over device tensors (pfsoft_batch_*)."""
+
+    def __init__(self, lib, bws, flags, tpc=0):
+        import ctypes
+        self.lib, self.n = lib, len(bws)
+        self.h = ctypes.c_void_p()
+        arr = (ctypes.c_int * len(bws))(*bws)
+        assert lib.pfsoft_batch_create(arr, len(bws), tpc, flags, ctypes.byref(self.h)) == 0, lib.pfsoft_last_error()
+
+    def _ptrs(self, ts):
+        import ctypes
+        return (ctypes.c_void_p * self.n)(*[t.data_ptr() for t in ts])
+
+    def idsoft(self, coeffs, grids, s):
+        assert self.lib.pfsoft_batch_idsoft(self.h, self._ptrs(coeffs), self._ptrs(grids), s) == 0
+
+    def dsoft(self, grids, coeffs, s):
+        assert self.lib.pfsoft_batch_dsoft(self.h, self._ptrs(grids), self._ptrs(coeffs), s) == 0
+
+    def status(self):
+        return self.lib.pfsoft_batch_status(self.h)
+
+    def close(self):
+        if self.h:
+            self.lib.pfsoft_batch_destroy(self.h)
+            self.h = None
+
+
+def mixed_section(lib, steps: int, warmup: int, tune: bool = False) -> dict:
+    """256 independent transforms, bandwidths uniform over {32,48,64,96,128} (PCG64 seed 2),
+    |f| = (1+l)^-1.5 with uniform phase (device generator, seed 2000 + i). One step = IDSOFT then
+    DSOFT of every transform, for: the plain loop over the single-transform entry points (FP64),
+    the FP64 batch plan (one fused DWT launch per direction, CUDA graph), the split-precision batch
+    plan (one tcgen05 launch per direction), and the split-precision server, saturated (all 512
+    requests submitted at once). Errors: split against FP64 for every transform, and the first
+    B = 32 transform's split results against the long-double oracle."""
+    import numpy as np
+    import torch
+
+    from oracle import oracle as orc
+    from pfsoftlib_b200 import autotune
+    from pfsoftlib_b200.serving import TransformServer
+
+    s = torch.cuda.current_stream().cuda_stream
+    rng = np.random.default_rng(2)
+    bws = [int(b) for b in rng.choice(MIXED_BANDS, size=256)]
+    coeffs = [_dev_coeffs(lib, Bi, 2000 + i, 2, 1.5, s) for i, Bi in enumerate(bws)]
+    grids = [torch.empty((2 * Bi,) * 3, dtype=torch.complex128, device="cuda") for Bi in bws]
+    back = [torch.empty_like(c) for c in coeffs]
+    ws = torch.empty(lib.pfsoft_workspace_bytes(max(bws)) // 8, dtype=torch.float64, device="cuda")
+
+    def plain():
+        for i, Bi in enumerate(bws):
+            assert lib.pfsoft_cuda_idsoft(coeffs[i].data_ptr(), Bi, grids[i].data_ptr(), ws.data_ptr(), ws.numel() * 8, s) == 0
+            assert lib.pfsoft_cuda_dsoft(grids[i].data_ptr(), Bi, back[i].data_ptr(), ws.data_ptr(), ws.numel() * 8, s) == 0
+
+    ms_plain = _timed(plain, steps, warmup)
+    g64 = [g.clone() for g in grids]
+    c64 = [b.clone() for b in back]
+    del ws
+    tpc, tune_ms = 0, None
+    if tune:
+        tpc, tune_ms = autotune.tune_batch(lib, bws, coeffs, grids, back, use_cache=False)
+    p64 = _Plan(lib, bws, 0, tpc)
+    ms_batch = _timed(lambda: (p64.idsoft(coeffs, grids, s), p64.dsoft(grids, back, s)), steps, warmup)
+    batch_vs = max(_rel(back[i], c64[i]) for i in range(len(bws)))
+    p64.close()
+    psp = _Plan(lib, bws, SPLIT)
+    ms_split = _timed(lambda: (psp.idsoft(coeffs, grids, s), psp.dsoft(grids, back, s)), steps, warmup)
+    split_status = psp.status()
+    psp.close()
+    torch.cuda.synchronize()
+    split_grid_vs = max(_rel(grids[i], g64[i]) for i in range(len(bws)))
+    split_coef_vs = max(_rel(back[i], c64[i]) for i in range(len(bws)))
+    split_rt = max(_rel(back[i], coeffs[i]) for i in range(len(bws)))
+    # the oracle on the first B = 32 transform (long double, all on the host)
+    i32 = bws.index(32)
+    ora = orc.Oracle()
+    c_h = coeffs[i32].cpu().numpy()
+    g_h = grids[i32].cpu().numpy()
+    oracle_grid = orc.rel_l2(g_h, ora.idsoft(c_h, 32))
+    oracle_coef = orc.rel_l2(back[i32].cpu().numpy(), ora.dsoft(g_h))
+    # the split-precision server, saturated: all 512 requests at once, fresh outputs
+    out_g = [torch.empty_like(g) for g in grids]
+    out_c = [torch.empty_like(c) for c in coeffs]
+    jobs = [(1, i) for i in range(len(bws))] + [(0, i) for i in range(len(bws))]
+    order = np.random.default_rng(3).permutation(len(jobs))
+    torch.cuda.synchronize()
+    with TransformServer(budget_bytes=48 << 30, max_batch=16, streams=4, split=True) as srv:
+        def submit(j):
+            d, i = jobs[j]
+            return srv.idsoft(coeffs[i], out_g[i]) if d == 1 else srv.dsoft(g64[i], out_c[i])
+        for r in [submit(j) for j in order[:64]]:    # warm-up
+            r.wait(300)
+        srv.reset_stats()
+        for r in [submit(j) for j in order]:
+            r.wait(300)
+        sat = srv.stats()
+    served_vs = max(max(_rel(out_c[i], c64[i]), _rel(out_g[i], g64[i])) for i in range(len(bws)))
+    n = 2 * len(bws)
+    tps = lambda ms: n / (ms / 1e3)
+    return {
+        "workload": "256 transforms, B uniform over {32,48,64,96,128} (seed 2), |f|=(1+l)^-1.5; "
+                    "one step = IDSOFT + DSOFT of all",
+        "bandwidth_counts": {str(b): bws.count(b) for b in MIXED_BANDS},
+        "plain_loop": {"value": tps(ms_plain), "ms_per_step": ms_plain},
+        "fp64_batch": {"value": tps(ms_batch), "ms_per_step": ms_batch, "speedup_vs_plain_loop": ms_plain / ms_batch,
+                       "rel_l2_vs_plain_max": batch_vs, "transforms_per_cta": tpc or "default", "autotune_ms": tune_ms},
+        "split_batch": {"value": tps(ms_split), "ms_per_step": ms_split, "speedup_vs_plain_loop": ms_plain / ms_split,
+                        "status": split_status},
+        "split_served": {"value": sat["transforms_per_s"], "speedup_vs_plain_loop": sat["transforms_per_s"] / tps(ms_plain),
+                         "p50_ms": sat["p50_ms"], "p99_ms": sat["p99_ms"], "mean_batch": sat["mean_batch"],
+                         "max_concurrent_batches": sat["max_concurrent_batches"],
+                         "timing": "host clock, first submit -> last completion, 512 requests submitted at once"},
+        "accuracy": {"split_grid_rel_l2_vs_fp64_max": split_grid_vs, "split_coef_rel_l2_vs_fp64_max": split_coef_vs,
+                     "split_round_trip_rel_l2_max": split_rt, "served_rel_l2_vs_fp64_max": served_vs,
+                     "split_vs_oracle_B32": {"grid_rel_l2": oracle_grid, "coef_rel_l2": oracle_coef}},
+        "steps": steps, "warmup": max(1, warmup),
+    }
+
+
+def run_mixed(args):
+    import torch
+
+    import pfsoftlib_b200
+
+    lib = pfsoftlib_b200.load()
+    torch.cuda.set_device(0)
+    steps = max(1, min(args.steps, 5))
+    clocks = ClockSampler(0)
+    clocks.start()
+    sec = mixed_section(lib, steps, args.warmup, tune=True)
+    clk = clocks.stop()
+    line = {
+        "metric": "DSOFT+iDSOFT transforms/s, 256 transforms of uneven bandwidth (split-precision batch)",
+        "value": sec["split_batch"]["value"], "unit": "transforms/s", "n_gpus": 1, "steps": steps,
+        "warmup": max(1, args.warmup), "ms_per_step": sec["split_batch"]["ms_per_step"], "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64 data; s8 digit products, exact s32 sums, f64 combine",
+        "data": "synthetic (device generator)",
+        "config": {"workload": sec["workload"], "l2": "working set ~45 GB, far above L2"},
+        "mixed": sec, "clocks": clk,
+    }
+    print(json.dumps(line), flush=True)
+
+
+def b256_section(lib, groups: int = 1, check_reference: bool = True) -> dict:
+    """Transforms at B = 256 (|f| = (1+l)^-2 with uniform phase, device generator, seed 3 + i) in
+    groups of 8 through one batch plan: IDSOFT (8 grids of 2.15 GB) then DSOFT of those grids, FP64
+    plan (per-transform FP64 DWT above B = 128) against the split-precision plan (one tcgen05 launch
+    per direction). Errors: split against FP64, the split round trip, and the last group's first
+    split DSOFT against the compiled reference's CPU DSOFT of the same grid (all host threads)."""
+    import torch
+
+    from oracle import oracle as orc
+
+    s = torch.cuda.current_stream().cuda_stream
+    Bb, G = 256, 8
+    coeffs = [torch.empty(Bb * (4 * Bb * Bb - 1) // 3, dtype=torch.complex128, device="cuda") for _ in range(G)]
+    grids = [torch.empty((2 * Bb,) * 3, dtype=torch.complex128, device="cuda") for _ in range(G)]
+    back = [torch.empty_like(c) for c in coeffs]
+    ms = {}
+    worst = {"split_grid_rel_l2_vs_fp64_max": 0.0, "split_coef_rel_l2_vs_fp64_max": 0.0, "split_round_trip_rel_l2_max": 0.0,
+             "fp64_round_trip_rel_l2_max": 0.0}
+    plans = {"fp64": _Plan(lib, [Bb] * G, 0), "split": _Plan(lib, [Bb] * G, SPLIT)}
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    status = 0
+    for g0 in range(0, G * (groups + 1), G):   # the first group is the warm-up
+        for i in range(G):
+            assert lib.pfsoft_cuda_random_coeffs(coeffs[i].data_ptr(), Bb, 3 + g0 + i, 2, 2.0, s) == 0
+        res = {}
+        for name, p in plans.items():
+            torch.cuda.synchronize()
+            e0.record()
+            p.idsoft(coeffs, grids, s)
+            p.dsoft(grids, back, s)
+            e1.record()
+            torch.cuda.synchronize()
+            if g0 > 0:
+                ms[name] = ms.get(name, 0.0) + e0.elapsed_time(e1)
+            if name == "fp64":
+                res["g"] = [g.clone() for g in grids]
+                res["c"] = [b.clone() for b in back]
+                worst["fp64_round_trip_rel_l2_max"] = max(worst["fp64_round_trip_rel_l2_max"],
+                                                          max(_rel(back[i], coeffs[i]) for i in range(G)))
+        status |= plans["split"].status()
+        for i in range(G):
+            worst["split_grid_rel_l2_vs_fp64_max"] = max(worst["split_grid_rel_l2_vs_fp64_max"], _rel(grids[i], res["g"][i]))
+            worst["split_coef_rel_l2_vs_fp64_max"] = max(worst["split_coef_rel_l2_vs_fp64_max"], _rel(back[i], res["c"][i]))
+            worst["split_round_trip_rel_l2_max"] = max(worst["split_round_trip_rel_l2_max"], _rel(back[i], coeffs[i]))
+        del res
+    for p in plans.values():
+        p.close()
+    acc = dict(worst)
+    if check_reference and orc.Reference.available():
+        ref = orc.Reference()
+        g_h = grids[0].cpu().numpy()
+        t0 = time.perf_counter()
+        f_ref = ref.dsoft(g_h, ref.max_threads())
+        acc["split_vs_reference_dsoft"] = {"rel_l2": orc.rel_l2(back[0].cpu().numpy(), f_ref),
+                                           "max_abs": orc.max_abs(back[0].cpu().numpy(), f_ref),
+                                           "reference_s": time.perf_counter() - t0, "threads": ref.max_threads()}
+        del g_h, f_ref
+    n = 2 * G * groups
+    return {
+        "workload": f"{G * groups} transforms at B=256 (seed 3+i, |f|=(1+l)^-2) in groups of 8 through one batch "
+                    f"plan; IDSOFT + DSOFT of each",
+        "fp64": {"value": n / (ms["fp64"] / 1e3), "ms": ms["fp64"]},
+        "split": {"value": n / (ms["split"] / 1e3), "ms": ms["split"], "speedup_vs_fp64": ms["fp64"] / ms["split"],
+                  "status": status},
+        "accuracy": acc,
+    }
+
+
+def run_b256(args):
+    import torch
+
+    import pfsoftlib_b200
+
+    lib = pfsoftlib_b200.load()
+    torch.cuda.set_device(0)
+    clocks = ClockSampler(0)
+    clocks.start()
+    sec = b256_section(lib, groups=8)
+    clk = clocks.stop()
+    line = {
+        "metric": "DSOFT+iDSOFT transforms/s, 64 transforms at B=256 (split precision)", "value": sec["split"]["value"],
+        "unit": "transforms/s", "n_gpus": 1, "steps": 1, "warmup": 1, "ms_per_step": sec["split"]["ms"],
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64 data; s8 digit products, exact s32 sums, f64 combine", "data": "synthetic (device generator)",
+        "config": {"workload": sec["workload"], "grid": "512^3 complex128 (2.15 GB) each", "l2": "far above L2"},
+        "b256": sec, "clocks": clk,
+    }
+    print(json.dumps(line), flush=True)
+
+
+def _log_uniform_bandwidths(rng, n, lo=16, hi=256):
+    """Integers lo..hi with P(B) proportional to log((B+1)/B) (a continuous log-uniform variate on
+    [lo, hi+1) rounded down)."""
+    import numpy as np
+    return np.minimum(hi, np.floor(np.exp(rng.uniform(np.log(lo), np.log(hi + 1), size=n)))).astype(int)
+
+
+def serving_section(lib, rates, seconds: float, budget_gb: float, seed: int = 4) -> dict:
+    """Poisson arrivals at each offered rate for `seconds`: requests 50/50 DSOFT / iDSOFT, bandwidth
+    log-uniform over the integers 16..256 (PCG64 `seed`). Inputs stay on the device: one seeded
+    B = 256 coefficient set (|f| = (1+l)^-1.5, uniform phase) and its grid; a request at bandwidth B
+    reads the leading B(4B^2-1)/3 coefficients (a complete coefficient set of bandwidth B, the packed
+    layout being degree-major) or the leading (2B)^3 grid values. Outputs go to pools of buffers,
+    a request waiting for its buffer's previous user. Two forms, one after the other:
+      split_served  TransformServer(split=True): batches of one direction and any bandwidths,
+                    split-precision DWT in one launch per batch, up to 4 batches in flight;
+      plain         the single-transform FP64 entry points, one request at a time in arrival order
+                    on one stream (latency from arrival to the completion event on the device).
+    Tables of every bandwidth are built in a warm-up pass first (the server builds a bandwidth's
+    tables at submission, outside the latency it reports)."""
     import numpy as np
     import torch
 
     from pfsoftlib_b200.serving import TransformServer
 
-    rng = np.random.default_rng(seed)
-    n = len(bws)
-    out_g = [torch.empty_like(g) for g in grids]
-    out_c = [torch.empty_like(c) for c in coeffs]
-    jobs = [(1, i) for i in range(n)] + [(0, i) for i in range(n)]
-    order = rng.permutation(len(jobs))
+    s = torch.cuda.current_stream().cuda_stream
+    BM = 256
+    coef_in = _dev_coeffs(lib, BM, 4000, 2, 1.5, s)
+    grid_in = torch.empty((2 * BM,) * 3, dtype=torch.complex128, device="cuda")
+    assert lib.pfsoft_cuda_idsoft(coef_in.data_ptr(), BM, grid_in.data_ptr(), None, 0, s) == 0
+    pool_g, pool_c = 12, 64
+    out_g = [torch.empty((2 * BM) ** 3, dtype=torch.complex128, device="cuda") for _ in range(pool_g)]
+    out_c = [torch.empty_like(coef_in) for _ in range(pool_c)]
+    ws = torch.empty(lib.pfsoft_workspace_bytes(BM) // 8, dtype=torch.float64, device="cuda")
     torch.cuda.synchronize()
+    ncoef = lambda b: b * (4 * b * b - 1) // 3
 
-    def submit(srv, j):
-        d, i = jobs[j]
-        if d == 1:
-            return srv.idsoft(coeffs[i], out_g[i])
-        return srv.dsoft(grids[i], out_c[i])
+    def views(d, b, k):
+        if d == 0:   # DSOFT: grid in, coefficients out
+            return grid_in.view(-1)[: (2 * b) ** 3], out_c[k % pool_c][: ncoef(b)]
+        return coef_in[: ncoef(b)], out_g[k % pool_g][: (2 * b) ** 3]
 
-    with TransformServer(budget_bytes=48 << 30, max_batch=16, streams=4) as srv:
-        reqs = [submit(srv, j) for j in order[:64]]          # warm-up: tables, item lists
-        for r in reqs:
-            r.wait()
-        srv.reset_stats()
-        reqs = [submit(srv, j) for j in order]
-        for r in reqs:
-            r.wait()
-        sat = srv.stats()
-        rate = 0.6 * sat["transforms_per_s"]
-        srv.reset_stats()
-        gaps = rng.exponential(1.0 / rate, size=len(jobs))
+    rng = np.random.default_rng(seed)
+    plan = []
+    for rate in rates:
+        n = max(20, int(rate * seconds))
+        plan.append((rate, _log_uniform_bandwidths(rng, n), rng.integers(0, 2, size=n), rng.exponential(1.0 / rate, size=n)))
+
+    free, _ = torch.cuda.mem_get_info()
+    budget = int(min(budget_gb * (1 << 30), free - (6 << 30)))
+    out = {"budget_bytes": budget, "requests_per_rate": [len(p[1]) for p in plan], "split_served": [], "plain": []}
+    with TransformServer(budget_bytes=budget, max_batch=16, streams=4, split=True) as srv:
+        # warm-up: every bandwidth once per direction (tables, first launches); its statistics are
+        # the cold-start figures
         t0 = time.perf_counter()
-        due = t0 + np.cumsum(gaps)
-        reqs = []
-        for k, j in enumerate(order):
-            while time.perf_counter() < due[k]:
+        warm = []
+        for b in range(16, BM + 1):
+            for d in (0, 1):
+                i, o = views(d, b, b)
+                warm.append(srv.submit(d, b, i, o))
+        for r in warm:
+            r.wait(600)
+        st = srv.stats()
+        out["cold_start"] = {"requests": len(warm), "seconds": time.perf_counter() - t0, "p50_ms": st["p50_ms"],
+                             "p99_ms": st["p99_ms"], "note": "all 482 submitted at once with no tables built"}
+        for rate, Bs, dirs, gaps in plan:
+            srv.reset_stats()
+            last = {}
+            due = time.perf_counter() + np.cumsum(gaps)
+            reqs = []
+            for k in range(len(Bs)):
+                b, d = int(Bs[k]), int(dirs[k])
+                slot = (d, k % (pool_c if d == 0 else pool_g))
+                if slot in last:
+                    last[slot].wait(600)      # the output buffer is free again
+                while time.perf_counter() < due[k]:
+                    pass
+                i, o = views(d, b, k)
+                r = srv.submit(d, b, i, o)
+                last[slot] = r
+                reqs.append(r)
+            for r in reqs:
+                r.wait(600)
+            st = srv.stats()
+            out["split_served"].append({"offered_per_s": rate, "transforms_per_s": st["transforms_per_s"],
+                                        "p50_ms": st["p50_ms"], "p99_ms": st["p99_ms"], "mean_ms": st["mean_ms"],
+                                        "max_ms": st["max_ms"], "mean_batch": st["mean_batch"],
+                                        "max_concurrent_batches": st["max_concurrent_batches"],
+                                        "peak_bytes": st["peak_bytes"], "failed": st["failed"]})
+    # the plain per-request FP64 path: one stream, arrival order
+    stream = torch.cuda.current_stream()
+    for rate, Bs, dirs, gaps in plan:
+        n = len(Bs)
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(n)]
+        start = torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        start.record(stream)
+        arrive = t0 + np.cumsum(gaps)
+        for k in range(n):
+            b, d = int(Bs[k]), int(dirs[k])
+            while time.perf_counter() < arrive[k]:
                 pass
-            reqs.append(submit(srv, j))
-        for r in reqs:
-            r.wait()
-        ol = srv.stats()
-    worst = 0.0
-    for i in range(n):
-        worst = max(worst, torch.linalg.vector_norm(out_c[i] - plain_back[i]).item()
-                    / torch.linalg.vector_norm(plain_back[i]).item())
-    keep = ("transforms_per_s", "p50_ms", "p99_ms", "mean_ms", "max_ms", "batches", "mean_batch",
-            "max_concurrent_batches", "peak_bytes")
-    plain_tps = 2 * n / (ms_plain / 1e3)
-    return {
-        "server": {"budget_bytes": 48 << 30, "max_batch": 16, "streams": 4},
-        "saturated": {k: sat[k] for k in keep},
-        "open_loop": dict({k: ol[k] for k in keep}, offered_per_s=rate),
-        "speedup_vs_plain_loop": sat["transforms_per_s"] / plain_tps,
-        "served_vs_plain_rel_l2_max": worst,
-        "timing": "host clock, submit -> completion callback on the server's stream",
-    }
-
-
-def run_mixed(args):
-    """256 independent transforms, bandwidths uniform over {32,48,64,96,128} (PCG64 seed 2),
-    |f| = (1+l)^-1.5 with uniform phase (device generator, seed 2000 + i). One step = IDSOFT then
-    DSOFT of every transform. Batched engine (one plan, one fused DWT launch per direction, CUDA
-    graph, autotuned) against looping the single-transform entry points over the same inputs."""
-    import ctypes
-
-    import numpy as np
-    import torch
-
-    import pfsoftlib_b200
-    from pfsoftlib_b200 import autotune
-
-    lib = pfsoftlib_b200.load()
-    torch.cuda.set_device(0)
-    s = torch.cuda.current_stream().cuda_stream
-    rng = np.random.default_rng(2)
-    bws = [int(b) for b in rng.choice(MIXED_BANDS, size=256)]
-    coeffs, grids, back = [], [], []
-    for i, B in enumerate(bws):
-        c = torch.empty(B * (4 * B * B - 1) // 3, dtype=torch.complex128, device="cuda")
-        assert lib.pfsoft_cuda_random_coeffs(c.data_ptr(), B, 2000 + i, 2, 1.5, s) == 0
-        coeffs.append(c)
-        grids.append(torch.empty((2 * B,) * 3, dtype=torch.complex128, device="cuda"))
-        back.append(torch.empty_like(c))
-    tpc, timings = autotune.tune_batch(lib, bws, coeffs, grids, back, use_cache=False)
-    plan = ctypes.c_void_p()
-    arr = (ctypes.c_int * len(bws))(*bws)
-    assert lib.pfsoft_batch_create(arr, len(bws), tpc, 0, ctypes.byref(plan)) == 0, lib.pfsoft_last_error()
-    cp = (ctypes.c_void_p * len(bws))(*[t.data_ptr() for t in coeffs])
-    gp = (ctypes.c_void_p * len(bws))(*[t.data_ptr() for t in grids])
-    bp = (ctypes.c_void_p * len(bws))(*[t.data_ptr() for t in back])
-
-    def batched():
-        assert lib.pfsoft_batch_idsoft(plan, cp, gp, s) == 0
-        assert lib.pfsoft_batch_dsoft(plan, gp, bp, s) == 0
-
-    ws = torch.empty(lib.pfsoft_workspace_bytes(max(bws)) // 8, dtype=torch.float64, device="cuda")
-
-    def plain():
-        for i, B in enumerate(bws):
-            assert lib.pfsoft_cuda_idsoft(coeffs[i].data_ptr(), B, grids[i].data_ptr(), ws.data_ptr(), ws.numel() * 8, s) == 0
-            assert lib.pfsoft_cuda_dsoft(grids[i].data_ptr(), B, back[i].data_ptr(), ws.data_ptr(), ws.numel() * 8, s) == 0
-
-    def timed(fn, steps):
-        for _ in range(max(1, args.warmup)):
-            fn()
+            i, o = views(d, b, k)
+            f = lib.pfsoft_cuda_dsoft if d == 0 else lib.pfsoft_cuda_idsoft
+            assert f(i.data_ptr(), b, o.data_ptr(), ws.data_ptr(), ws.numel() * 8, s) == 0
+            ev[k].record(stream)
         torch.cuda.synchronize()
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record()
-        for _ in range(steps):
-            fn()
-        e1.record()
-        torch.cuda.synchronize()
-        return e0.elapsed_time(e1) / steps
-
-    steps = max(1, min(args.steps, 5))
-    clocks = ClockSampler(0)
-    clocks.start()
-    ms_plain = timed(plain, steps)
-    plain_back = [b.clone() for b in back]
-    ms_batch = timed(batched, steps)
-    clk = clocks.stop()
-    # accuracy: round trip of the batched engine, and batched vs plain on the same inputs
-    worst_rt, worst_vs = 0.0, 0.0
-    for i in range(len(bws)):
-        d = (back[i] - coeffs[i]).abs().max().item()
-        worst_rt = max(worst_rt, d)
-        nrm = torch.linalg.vector_norm(plain_back[i]).item()
-        worst_vs = max(worst_vs, torch.linalg.vector_norm(back[i] - plain_back[i]).item() / nrm)
-    lib.pfsoft_batch_destroy(plan)
-    # the same batch with the split-precision tensor-core DWT
-    plan_s = ctypes.c_void_p()
-    assert lib.pfsoft_batch_create(arr, len(bws), tpc, 2, ctypes.byref(plan_s)) == 0, lib.pfsoft_last_error()
-
-    def split():
-        assert lib.pfsoft_batch_idsoft(plan_s, cp, gp, s) == 0
-        assert lib.pfsoft_batch_dsoft(plan_s, gp, bp, s) == 0
-
-    ms_split = timed(split, steps)
-    split_status = lib.pfsoft_batch_status(plan_s)
-    lib.pfsoft_batch_destroy(plan_s)
-    split_vs, split_rt = 0.0, 0.0
-    for i in range(len(bws)):
-        split_vs = max(split_vs, (torch.linalg.vector_norm(back[i] - plain_back[i]) / torch.linalg.vector_norm(plain_back[i])).item())
-        split_rt = max(split_rt, (torch.linalg.vector_norm(back[i] - coeffs[i]) / torch.linalg.vector_norm(coeffs[i])).item())
-    served = run_served(lib, bws, coeffs, grids, plain_back, ms_plain)
-    n = 2 * len(bws)
-    line = {
-        "metric": "DSOFT+iDSOFT transforms/s, 256 transforms of uneven bandwidth", "value": n / (ms_batch / 1e3),
-        "unit": "transforms/s", "n_gpus": 1, "steps": steps, "warmup": max(1, args.warmup),
-        "ms_per_step": ms_batch, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-        "data": "synthetic (device generator)",
-        "config": {"workload": "256 transforms, B uniform over {32,48,64,96,128} (seed 2), |f|=(1+l)^-1.5, "
-                               "one step = IDSOFT + DSOFT of all", "bandwidth_counts": {str(b): bws.count(b) for b in MIXED_BANDS},
-                   "l2": "working set ~45 GB, far above L2"},
-        "plain_loop": {"value": n / (ms_plain / 1e3), "ms_per_step": ms_plain},
-        "speedup_vs_plain_loop": ms_plain / ms_batch,
-        "split_precision": {"value": n / (ms_split / 1e3), "ms_per_step": ms_split,
-                            "speedup_vs_plain_loop": ms_plain / ms_split, "rel_l2_vs_fp64_max": split_vs,
-                            "round_trip_rel_l2_max": split_rt, "status": split_status,
-                            "note": "DWT as bf16 digit-plane products on tcgen05, FP32 accumulation, FP64 sum"},
-        "served": served,
-        "autotune": {"transforms_per_cta": tpc, "round_trip_ms": timings},
-        "accuracy": {"round_trip_max_abs": worst_rt, "batched_vs_plain_rel_l2_max": worst_vs},
-        "clocks": clk,
-    }
-    print(json.dumps(line), flush=True)
+        done_ms = np.array([start.elapsed_time(e) for e in ev])
+        lat = done_ms - 1e3 * (arrive - t0)
+        span = done_ms[-1] - 1e3 * (arrive[0] - t0)
+        out["plain"].append({"offered_per_s": rate, "transforms_per_s": n / (span / 1e3),
+                             "p50_ms": float(np.percentile(lat, 50, method="higher")),
+                             "p99_ms": float(np.percentile(lat, 99, method="higher")),
+                             "mean_ms": float(lat.mean()), "max_ms": float(lat.max())})
+    return out
 
 
-def run_b256(args):
-    """64 transforms at B = 256 (|f| = (1+l)^-2 with uniform phase, device generator, seed 3 + i),
-    streamed through one batch plan in groups of 8: per group the coefficients are generated, then
-    IDSOFT (8 grids of 2.15 GB) and DSOFT of those grids. One step = all 64 IDSOFT + DSOFT; the
-    generation is outside the timed region. Accuracy: round trip of every transform, and the first
-    grid of the last group against the compiled reference's CPU DSOFT (all host threads) when it is
-    built."""
-    import ctypes
-
+def run_serve_sweep(args):
     import torch
 
     import pfsoftlib_b200
 
     lib = pfsoftlib_b200.load()
     torch.cuda.set_device(0)
-    s = torch.cuda.current_stream().cuda_stream
-    B, G, T = 256, 8, 64
-    n = B * (4 * B * B - 1) // 3
-    coeffs = [torch.empty(n, dtype=torch.complex128, device="cuda") for _ in range(G)]
-    grids = [torch.empty((2 * B,) * 3, dtype=torch.complex128, device="cuda") for _ in range(G)]
-    back = [torch.empty_like(c) for c in coeffs]
-    plan = ctypes.c_void_p()
-    assert lib.pfsoft_batch_create((ctypes.c_int * G)(*[B] * G), G, 0, 0, ctypes.byref(plan)) == 0, lib.pfsoft_last_error()
-    cp = (ctypes.c_void_p * G)(*[t.data_ptr() for t in coeffs])
-    gp = (ctypes.c_void_p * G)(*[t.data_ptr() for t in grids])
-    bp = (ctypes.c_void_p * G)(*[t.data_ptr() for t in back])
-    worst = [0.0]
-
-    def group(g0, check):
-        for i in range(G):
-            assert lib.pfsoft_cuda_random_coeffs(coeffs[i].data_ptr(), B, 3 + g0 + i, 2, 2.0, s) == 0
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record()
-        assert lib.pfsoft_batch_idsoft(plan, cp, gp, s) == 0
-        assert lib.pfsoft_batch_dsoft(plan, gp, bp, s) == 0
-        e1.record()
-        torch.cuda.synchronize()
-        if check:
-            for c, b in zip(coeffs, back):
-                worst[0] = max(worst[0], (torch.linalg.vector_norm(b - c) / torch.linalg.vector_norm(c)).item())
-        return e0.elapsed_time(e1)
-
-    group(0, False)   # warm-up: tables, plan graph
-    steps = max(1, min(args.steps, 2))
+    rates = [float(r) for r in args.rates.split(",") if r]
     clocks = ClockSampler(0)
     clocks.start()
-    ms = 0.0
-    for _ in range(steps):
-        for g0 in range(0, T, G):
-            ms += group(g0, True)
+    sec = serving_section(lib, rates, args.seconds, args.budget_gb)
     clk = clocks.stop()
-    lib.pfsoft_batch_destroy(plan)
-    ms /= steps
-    acc = {"round_trip_rel_l2_max": worst[0]}
-    # checker: the compiled reference's CPU DSOFT of the last group's first grid, all host threads
-    from oracle import oracle as orc
-    if orc.Reference.available():
-        ref = orc.Reference()
-        g_h = grids[0].cpu().numpy()
-        t0 = time.perf_counter()
-        f_ref = ref.dsoft(g_h, ref.max_threads())
-        acc["vs_reference_dsoft_rel_l2"] = orc.rel_l2(back[0].cpu().numpy(), f_ref)
-        acc["vs_reference_dsoft_max_abs"] = orc.max_abs(back[0].cpu().numpy(), f_ref)
-        acc["reference_dsoft_s"] = time.perf_counter() - t0
-        acc["reference_threads"] = ref.max_threads()
-        del g_h, f_ref
+    best = max(x["transforms_per_s"] for x in sec["split_served"])
     line = {
-        "metric": "DSOFT+iDSOFT transforms/s, 64 transforms at B=256", "value": 2 * T / (ms / 1e3),
-        "unit": "transforms/s", "n_gpus": 1, "steps": steps, "warmup": 1, "ms_per_step": ms,
-        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "metric": "served DSOFT/iDSOFT transforms/s under Poisson arrivals, split precision (best over the sweep)",
+        "value": best, "unit": "transforms/s", "n_gpus": 1, "steps": len(rates), "warmup": 1, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64 data; s8 digit products, exact s32 sums, f64 combine",
         "data": "synthetic (device generator)",
-        "config": {"workload": "64 transforms at B=256 (seed 3+i, |f|=(1+l)^-2), groups of 8 through one "
-                               "batch plan; one step = IDSOFT + DSOFT of all 64",
-                   "grid": "512^3 complex128 (2.15 GB) each", "l2": "far above L2"},
-        "accuracy": acc,
-        "split_precision": "not run: the split-precision DWT covers B = 16..128 (K <= 256 keeps its "
-                           "leading digit-plane sums exact in FP32)",
-        "clocks": clk,
+        "config": {"workload": "requests 50/50 DSOFT/iDSOFT, B log-uniform over the integers 16..256 (seed 4), "
+                               "Poisson arrivals", "rates": rates, "seconds_per_rate": args.seconds,
+                   "max_batch": 16, "streams": 4},
+        "serving": sec, "clocks": clk,
     }
     print(json.dumps(line), flush=True)
 
@@ -541,91 +716,6 @@ def run_shard(args):
     del st
     dist.destroy_process_group()
 
-
-SERVE_BANDS = (16, 24, 32, 48, 64, 96, 128, 192, 256)   # log-spaced: equal weights = log-uniform
-
-
-def run_serve_sweep(args):
-    """Serving under Poisson arrivals: requests 50/50 DSOFT / iDSOFT, bandwidth log-uniform over
-    16..256 (on the log-spaced grid SERVE_BANDS, PCG64 seed 4), offered at each rate of --rates for
-    --seconds. Inputs per bandwidth are generated once on the device; each request writes one of
-    four output buffers of its (bandwidth, direction), and waits for that buffer's previous request
-    before reusing it. Per rate: achieved transforms/s and p50 / p99 latency (submit -> result,
-    host clock at the server's completion callback)."""
-    import numpy as np
-    import torch
-
-    import pfsoftlib_b200
-    from pfsoftlib_b200.serving import TransformServer
-
-    lib = pfsoftlib_b200.load()
-    torch.cuda.set_device(0)
-    s = torch.cuda.current_stream().cuda_stream
-    pool = 4
-    ins, outs = {}, {}
-    for B in SERVE_BANDS:
-        c = torch.empty(B * (4 * B * B - 1) // 3, dtype=torch.complex128, device="cuda")
-        assert lib.pfsoft_cuda_random_coeffs(c.data_ptr(), B, 4000 + B, 2, 1.5, s) == 0
-        g = torch.empty((2 * B,) * 3, dtype=torch.complex128, device="cuda")
-        assert lib.pfsoft_cuda_idsoft(c.data_ptr(), B, g.data_ptr(), None, 0, s) == 0
-        ins[B] = (g, c)                     # direction 0 reads the grid, 1 the coefficients
-        outs[B] = ([torch.empty_like(c) for _ in range(pool)], [torch.empty_like(g) for _ in range(pool)])
-    torch.cuda.synchronize()
-    rng = np.random.default_rng(4)
-    rates = [float(r) for r in args.rates.split(",") if r]
-    sweep = []
-    # the arena is one allocation of the whole budget: cap it by what the device has left after
-    # the request buffers above (4 GiB kept back for tables, staging and the CUDA context)
-    free, _ = torch.cuda.mem_get_info()
-    budget = min(int(args.budget_gb * (1 << 30)), free - (4 << 30))
-    with TransformServer(budget_bytes=budget, max_batch=16, streams=4) as srv:
-        # warm-up: tables and item lists of every bandwidth and direction
-        warm = [srv.submit(d, B, ins[B][d], outs[B][d][0]) for B in SERVE_BANDS for d in (0, 1)]
-        for r in warm:
-            r.wait(300)
-        for rate in rates:
-            n = max(20, int(rate * args.seconds))
-            Bs = rng.choice(SERVE_BANDS, size=n)
-            dirs = rng.integers(0, 2, size=n)
-            gaps = rng.exponential(1.0 / rate, size=n)
-            slot = {}
-            last = {}
-            srv.reset_stats()
-            t0 = time.perf_counter()
-            due = t0 + np.cumsum(gaps)
-            reqs = []
-            for i in range(n):
-                B, d = int(Bs[i]), int(dirs[i])
-                k = slot.get((B, d), 0)
-                slot[(B, d)] = (k + 1) % pool
-                prev = last.get((B, d, k))
-                if prev is not None:
-                    prev.wait(300)                 # the output buffer is free again
-                while time.perf_counter() < due[i]:
-                    pass
-                r = srv.submit(d, B, ins[B][d], outs[B][d][k])
-                last[(B, d, k)] = r
-                reqs.append(r)
-            for r in reqs:
-                r.wait(300)
-            st = srv.stats()
-            sweep.append({"offered_per_s": rate, "requests": n, "transforms_per_s": st["transforms_per_s"],
-                          "p50_ms": st["p50_ms"], "p99_ms": st["p99_ms"], "mean_ms": st["mean_ms"],
-                          "max_ms": st["max_ms"], "mean_batch": st["mean_batch"],
-                          "max_concurrent_batches": st["max_concurrent_batches"], "peak_bytes": st["peak_bytes"]})
-            print(json.dumps({"rate": rate, **sweep[-1]}), file=sys.stderr, flush=True)
-    best = max(x["transforms_per_s"] for x in sweep)
-    line = {
-        "metric": "served DSOFT/iDSOFT transforms/s under Poisson arrivals (best over the sweep)", "value": best,
-        "unit": "transforms/s", "n_gpus": 1, "steps": len(rates), "warmup": 1, "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (device generator)",
-        "config": {"workload": "requests 50/50 DSOFT/iDSOFT, B log-uniform over 16..256 on "
-                               f"{list(SERVE_BANDS)} (seed 4), Poisson arrivals", "rates": rates,
-                   "seconds_per_rate": args.seconds, "budget_bytes": budget, "max_batch": 16, "streams": 4,
-                   "output_buffers_per_bandwidth_and_direction": pool},
-        "sweep": sweep,
-    }
-    print(json.dumps(line), flush=True)
 
 
 def main():
@@ -725,9 +815,12 @@ def main():
 
     # ---- accuracy of the timed results (round trip at B = 128)
     f_h = f.cpu().numpy()
-    acc = {"round_trip_rel_l2": orc.rel_l2(f_h, coeffs_h), "round_trip_max_abs": orc.max_abs(f_h, coeffs_h)}
+    acc = {"round_trip_rel_l2": orc.rel_l2(f_h, coeffs_h), "round_trip_max_abs": orc.max_abs(f_h, coeffs_h),
+           "round_trip_rel_l2_max_bound": 1e-13}
 
     # ---- per-stage roofline
+    peaks = measured_peaks()
+    hbm = peaks["hbm_gbs"]
     stages = {}
     for i in range(nstages):
         name = lib.pfsoft_profile_stage_name(i).decode()
@@ -737,7 +830,7 @@ def main():
         if name.startswith("fft"):
             achieved = FFT_PASS_BYTES / (per / 1e3) / 1e9
             stages[name] = {"bound": "hbm", "ms_per_launch": per, "launches": int(st_cnt[i]),
-                            "achieved": achieved, "peak": 6551.7, "unit": "GB/s", "frac": achieved / 6551.7}
+                            "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm}
         elif name.startswith("dwt"):
             achieved = DWT_FLOPS / (per / 1e3) / 1e12
             stages[name] = {"bound": "tensor", "ms_per_launch": per, "launches": int(st_cnt[i]),
@@ -747,15 +840,15 @@ def main():
             stages[name] = {"ms_per_launch": per, "launches": int(st_cnt[i])}
     dominant = max((k for k in stages if "frac" in stages[k]), key=lambda k: stages[k]["ms_per_launch"] * stages[k]["launches"])
     d = stages[dominant]
-    # DRAM bytes per launch (read + write) from one ncu capture of the same kernels at B = 128,
-    # profiles/dwt_single_b128.md and profiles/fft_pass_b128.md
+    # DRAM bytes per launch (read + write) of these kernels at B = 128, from one ncu capture of the
+    # same launches (dram__bytes_read.sum + dram__bytes_write.sum)
     traffic = {"dwt_forward": 268.37e6 + 43.51e6, "dwt_inverse": 46.44e6 + 208.20e6,
                "fft_forward_gamma": 268.5e6 + 221.6e6, "fft_inverse_alpha": 268.5e6 + 214.7e6,
                "fft_inverse_gamma": 268.5e6 + 219.7e6}
     roofline = {"kernel": dominant, "bound": d["bound"], "achieved": d["achieved"], "peak": d["peak"],
                 "unit": d["unit"], "frac": d["frac"], "traffic": traffic.get(dominant),
                 "peak_source": ("measured FP64 MMA peak (own micro-benchmark; MEASURED_PEAKS.json has no FP64 entry)"
-                                if d["bound"] == "tensor" else "measured copy bandwidth, MEASURED_PEAKS.json hbm_gbs")}
+                                if d["bound"] == "tensor" else peaks["source"])}
 
     # ---- end to end through the host-facing C ABI (pinned host buffers)
     ch = torch.from_numpy(coeffs_h).pin_memory()
@@ -774,14 +867,74 @@ def main():
     t0 = time.perf_counter()
     for _ in range(e2e_steps):
         host_step()
+    t_seq = time.perf_counter() - t0
+    # concurrent: one host thread runs the iDSOFTs, another the DSOFTs (of a grid already on the
+    # host), so that each step's device-to-host grid copy overlaps the other call's host-to-device
+    # grid copy (the PCIe link is full duplex; each call has its own staging buffers and stream)
+    import threading
+
+    gin = gh.clone().pin_memory()
+    gout = torch.empty_like(gh).pin_memory()
+    fout = torch.empty_like(fh).pin_memory()
+    errs = []
+
+    def worker(fn):
+        try:
+            for _ in range(e2e_steps):
+                if fn():
+                    raise RuntimeError(lib.pfsoft_last_error().decode())
+        except Exception as exc:   # surfaced below
+            errs.append(exc)
+
+    inv = lambda: lib.pfsoft_idsoft_host(ch.data_ptr(), B, gout.data_ptr())
+    fwd = lambda: lib.pfsoft_dsoft_host(gin.data_ptr(), B, fout.data_ptr())
+    inv()
+    fwd()
+    barrier()
+    t0 = time.perf_counter()
+    th = [threading.Thread(target=worker, args=(f,)) for f in (inv, fwd)]
+    for x in th:
+        x.start()
+    for x in th:
+        x.join()
     t_e2e = time.perf_counter() - t0
+    if errs:
+        raise errs[0]
     if dist is not None:
-        t = torch.tensor([t_e2e], dtype=torch.float64, device="cuda")
+        t = torch.tensor([t_e2e, t_seq], dtype=torch.float64, device="cuda")
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        t_e2e = float(t.item())
+        t_e2e, t_seq = float(t[0].item()), float(t[1].item())
     e2e = {"value": TRANSFORMS_PER_STEP * e2e_steps * world / t_e2e, "unit": UNIT,
            "h2d_bytes_per_step": COEF_BYTES + GRID_BYTES, "d2h_bytes_per_step": GRID_BYTES + COEF_BYTES,
-           "api": "pfsoft_idsoft_host + pfsoft_dsoft_host (include/pfsoft_b200.h), pinned host buffers", "steps": e2e_steps}
+           "api": "pfsoft_idsoft_host and pfsoft_dsoft_host (include/pfsoft_b200.h) from two host threads, one "
+                  "call of each in flight, pinned host buffers",
+           "steps": e2e_steps}
+    e2e_sequential = {"value": TRANSFORMS_PER_STEP * e2e_steps * world / t_seq, "unit": UNIT, "steps": e2e_steps,
+                      "api": "pfsoft_idsoft_host then pfsoft_dsoft_host of its grid, one thread, pinned host buffers"}
+    fout_check = orc.rel_l2(fout.numpy(), coeffs_h)
+    del gin, gout, fout
+    # the same on pageable host memory (what the C++ drop-in header passes: grid3D's new[] storage)
+    chp = coeffs_h.copy()
+    ghp = np.empty((N, N, N), dtype=np.complex128)
+    fhp = np.empty_like(chp)
+
+    def host_step_pageable():
+        rc = lib.pfsoft_idsoft_host(chp.ctypes.data, B, ghp.ctypes.data)
+        rc |= lib.pfsoft_dsoft_host(ghp.ctypes.data, B, fhp.ctypes.data)
+        if rc:
+            raise RuntimeError(lib.pfsoft_last_error().decode())
+
+    host_step_pageable()
+    barrier()
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        host_step_pageable()
+    t_pg = time.perf_counter() - t0
+    acc["host_round_trip_rel_l2"] = fout_check
+    e2e_pageable = {"value": TRANSFORMS_PER_STEP * e2e_steps / t_pg, "unit": UNIT, "steps": e2e_steps,
+                    "h2d_bytes_per_step": COEF_BYTES + GRID_BYTES, "d2h_bytes_per_step": GRID_BYTES + COEF_BYTES,
+                    "api": "pfsoft_idsoft_host + pfsoft_dsoft_host on pageable numpy buffers"}
+    del chp, ghp, fhp
 
     # ---- CPU baseline (rank 0, N = 1 only)
     cpu = None
@@ -805,11 +958,33 @@ def main():
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": max(3, args.warmup), "ms_per_step": ms / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": workload_config("inputs larger than L2: 268 MB grid and workspace, 45 MB coefficients"),
-        "e2e": e2e, "gpu_launches": int(launches), "roofline": roofline, "stages": stages,
-        "cpu_baseline": cpu, "accuracy": acc, "clocks": clk,
+        "config": workload_config(),
+        "e2e": e2e, "e2e_sequential": e2e_sequential, "e2e_pageable": e2e_pageable,
+        "gpu_launches": int(launches), "roofline": roofline,
+        "stages": stages, "cpu_baseline": cpu, "accuracy": acc, "clocks": clk,
         "parallelism": f"replicas x{world} (independent transforms per GPU, no collective)",
     }
+    # the other workloads, compact (N = 1 only): each section catches its own failure so that the
+    # headline line is still printed
+    if world == 1 and not args.no_extras:
+        del c, f, g, ws, ch, gh, fh
+        torch.cuda.empty_cache()
+        extras_clock = ClockSampler(local)
+        extras_clock.start()
+        t_x = time.perf_counter()
+        for key, fn in (("mixed", lambda: mixed_section(lib, 2, 1)),
+                        ("b256", lambda: b256_section(lib, groups=1)),
+                        ("serving", lambda: serving_section(lib, [100.0, 500.0, 1500.0], 1.5, 160.0))):
+            t_s = time.perf_counter()
+            try:
+                line[key] = fn()
+            except Exception as exc:   # reported, not hidden: the key carries the failure
+                line[key] = {"error": f"{type(exc).__name__}: {exc}"}
+            line[key]["section_s"] = time.perf_counter() - t_s
+            torch.cuda.synchronize()
+            torch.cuda.empty_cache()
+        line["extras_clocks"] = extras_clock.stop()
+        line["extras_s"] = time.perf_counter() - t_x
     print(json.dumps(line), flush=True)
 
 

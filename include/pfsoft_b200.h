@@ -112,7 +112,9 @@ int pfsoft_batch_idsoft(pfsoft_batch* batch, const double* const* d_coeffs, doub
 /* ---- Host-resident drop-in (synchronous) ---------------------------------------------------
  * The same transforms on host buffers: copy in, transform, copy out, wait. Pinned host
  * buffers (cudaHostAlloc) make the copies asynchronous DMA; pageable ones work too.
- * Calls on one device are serialised by the library (its staging buffers are shared). */
+ * Calls from different host threads run concurrently, each with its own device staging buffers
+ * and stream (a per-device pool, grown on demand and kept until exit), so one call's
+ * device-to-host copy can overlap another's host-to-device copy. */
 int pfsoft_dsoft_host(const double* h_grid, int B, double* h_coeffs);
 int pfsoft_idsoft_host(const double* h_coeffs, int B, double* h_grid);
 
@@ -163,7 +165,9 @@ int pfsoft_cuda_random_coeffs(double* d_coeffs, int B, unsigned long long seed, 
  *   direction 1: iDSOFT, d_in = coefficients, d_out = grid.
  * submit: `stream` is where the caller produced d_in (NULL: the legacy default stream): the
  *   request's batch waits for the work queued there before the call. The result is complete on
- *   the device once poll / wait report PFSOFT_OK.
+ *   the device once poll / wait report PFSOFT_OK. The first submission of a bandwidth on a device
+ *   builds its constant tables inside this call (on the server's own stream; the request's
+ *   latency counts from the end of the call).
  *   PFSOFT_ENOMEM if one transform of that bandwidth alone exceeds the budget (it is
  *   rejected, not queued); PFSOFT_EBUSY after the server began shutting down.
  * poll: PFSOFT_EBUSY while queued or running; otherwise the request's final status (PFSOFT_OK,

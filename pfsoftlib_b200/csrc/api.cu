@@ -47,6 +47,17 @@ int cuda_fail(cudaError_t e, const char* what)
 
 constexpr int kMaxBandwidth = 512;
 
+// Device buffers and stream of one host-staged call. A device keeps a pool of them, so that calls
+// from different host threads run concurrently (one's device-to-host copy overlapping another's
+// host-to-device copy on the two copy engines); a call takes a free context or makes one.
+struct StagingContext {
+    void* h_grid = nullptr;
+    void* h_coef = nullptr;
+    void* h_ws = nullptr;
+    size_t h_grid_bytes = 0, h_coef_bytes = 0, h_ws_bytes = 0;
+    cudaStream_t h_stream = nullptr;
+};
+
 struct DeviceState {
     std::mutex mu;
     std::map<int, BandTables> tables;
@@ -54,11 +65,28 @@ struct DeviceState {
     size_t ws_bytes = 0;
     // host-staged calls
     std::mutex host_mu;
-    void* h_grid = nullptr;
-    void* h_coef = nullptr;
-    void* h_ws = nullptr;
-    size_t h_grid_bytes = 0, h_coef_bytes = 0, h_ws_bytes = 0;
-    cudaStream_t h_stream = nullptr;
+    std::vector<StagingContext*> staging_free;
+};
+
+// Takes a staging context of the device (a free one, else a new one) and gives it back.
+struct StagingLease {
+    DeviceState* st;
+    StagingContext* ctx;
+    explicit StagingLease(DeviceState* s) : st(s), ctx(nullptr)
+    {
+        std::lock_guard<std::mutex> lk(st->host_mu);
+        if (!st->staging_free.empty()) {
+            ctx = st->staging_free.back();
+            st->staging_free.pop_back();
+        } else {
+            ctx = new StagingContext();   // lives until process exit
+        }
+    }
+    ~StagingLease()
+    {
+        std::lock_guard<std::mutex> lk(st->host_mu);
+        st->staging_free.push_back(ctx);
+    }
 };
 
 std::mutex g_devices_mu;
@@ -433,8 +461,8 @@ static int host_staged(int B, bool forward, const double* in, double* out)
     if (!in || !out) return fail(PFSOFT_EINVAL, "null host pointer");
     int dev = 0;
     PF_CUDA(cudaGetDevice(&dev));
-    DeviceState* st = device_state(dev);
-    std::lock_guard<std::mutex> lk(st->host_mu);
+    StagingLease lease(device_state(dev));
+    StagingContext* st = lease.ctx;
     const size_t gb = grid_elems(B) * sizeof(double2);
     const size_t cb = coef_offset(B) * sizeof(double2);
     if (!st->h_stream) PF_CUDA(cudaStreamCreateWithFlags(&st->h_stream, cudaStreamNonBlocking));
@@ -558,8 +586,8 @@ static int layer_wise_host(int cols, int rows, int lays, double* h_arr, double s
     if (!h_arr) return fail(PFSOFT_EINVAL, "null host pointer");
     int dev = 0;
     PF_CUDA(cudaGetDevice(&dev));
-    DeviceState* st = device_state(dev);
-    std::lock_guard<std::mutex> lk(st->host_mu);
+    StagingLease lease(device_state(dev));
+    StagingContext* st = lease.ctx;
     const size_t bytes = (size_t)cols * rows * lays * sizeof(double2);
     if (!st->h_stream) PF_CUDA(cudaStreamCreateWithFlags(&st->h_stream, cudaStreamNonBlocking));
     if (st->h_grid_bytes < bytes) {

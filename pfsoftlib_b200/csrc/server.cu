@@ -114,6 +114,7 @@ struct pfsoft_server {
     int max_batch = 16;
     bool split = false;          // PFSOFT_SERVER_SPLIT
     size_t stage_bytes = 0;
+    cudaStream_t table_stream = nullptr;   // builds a bandwidth's tables at submission
     std::vector<Slot> slots;
     void* arena_base = nullptr;
     pfsoft_serving::Arena arena;
@@ -459,6 +460,7 @@ int pfsoft_server_create_ex(size_t budget_bytes, int max_batch, int streams, int
     s->sched.set_mixed(s->split);
     cudaError_t e = cudaGetDevice(&s->device);
     if (e == cudaSuccess && s->split) e = dwt_split_prepare();
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&s->table_stream, cudaStreamNonBlocking);
     if (e == cudaSuccess) e = cudaMalloc(&s->arena_base, budget_bytes);
     s->arena.reset(e == cudaSuccess ? budget_bytes : 0, 256);
     s->slots.resize(streams);
@@ -488,6 +490,7 @@ int pfsoft_server_create_ex(size_t budget_bytes, int max_batch, int streams, int
             cudaFree(sl.d_counter);
             cudaFreeHost(sl.h_status);
         }
+        if (s->table_stream) cudaStreamDestroy(s->table_stream);
         cudaFree(s->arena_base);
         delete s;
         cudaGetLastError();
@@ -516,6 +519,7 @@ int pfsoft_server_destroy(pfsoft_server* s)
         cudaFreeHost(sl.h_status);
     }
     for (auto& kv : s->items) cudaFree(kv.second.first);
+    if (s->table_stream) cudaStreamDestroy(s->table_stream);
     for (cudaEvent_t ev : s->dead_events)
         if (ev) cudaEventDestroy(ev);
     cudaFree(s->arena_base);
@@ -542,6 +546,14 @@ int pfsoft_server_submit(pfsoft_server* s, int direction, int B, const double* d
             ++s->rejected;
             return fail(PFSOFT_ENOMEM, "one transform of this bandwidth exceeds the server's HBM budget");
         }
+    }
+    // the bandwidth's constant tables are built here, at admission (once per device and
+    // bandwidth, on the server's own stream), so that no batch waits for them and the request's
+    // latency, counted from the end of this call, does not include them
+    {
+        BandTables t;
+        const int rc = tables_for(B, s->table_stream, &t);
+        if (rc) return rc;
     }
     cudaEvent_t ready = nullptr;
     cudaError_t e = cudaEventCreateWithFlags(&ready, cudaEventDisableTiming);

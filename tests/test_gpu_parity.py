@@ -97,7 +97,7 @@ def test_round_trip_reference_criterion(lib, B):
 
 
 @pytest.mark.skipif(not orc.Reference.available(), reason="reference build (oracle/_ref) not present")
-@pytest.mark.parametrize("B", [32, 64])
+@pytest.mark.parametrize("B", [32, 64, 128])
 def test_matches_compiled_reference(lib, B):
     ref = orc.Reference()
     threads = ref.max_threads()
@@ -109,6 +109,45 @@ def test_matches_compiled_reference(lib, B):
     f_gpu, _ = gpu_dsoft(lib, g_ref, B)
     assert orc.rel_l2(f_gpu, f_ref) <= REL_TOL
     assert orc.max_abs(f_gpu, f_ref) <= ABS_TOL
+
+
+@pytest.mark.skipif(not orc.Reference.available(), reason="reference build (oracle/_ref) not present")
+@pytest.mark.parametrize("B", [192, 256])
+def test_forward_matches_compiled_reference_large(lib, B):
+    """DSOFT at B = 192 and 256 against the compiled reference's CPU DSOFT of the same grid (the
+    grid is the GPU iDSOFT of device-generated coefficients, |f| = (1+l)^-1 |N(0,1)|)."""
+    s = stream()
+    c = torch.empty(B * (4 * B * B - 1) // 3, dtype=torch.complex128, device="cuda")
+    assert lib.pfsoft_cuda_random_coeffs(c.data_ptr(), B, 77 + B, 1, 1.0, s) == 0
+    g = torch.empty((2 * B,) * 3, dtype=torch.complex128, device="cuda")
+    f = torch.empty_like(c)
+    assert lib.pfsoft_cuda_idsoft(c.data_ptr(), B, g.data_ptr(), None, 0, s) == 0
+    assert lib.pfsoft_cuda_dsoft(g.data_ptr(), B, f.data_ptr(), None, 0, s) == 0
+    torch.cuda.synchronize()
+    ref = orc.Reference()
+    f_ref = ref.dsoft(g.cpu().numpy(), ref.max_threads())
+    f_gpu = f.cpu().numpy()
+    assert orc.rel_l2(f_gpu, f_ref) <= REL_TOL
+    assert orc.max_abs(f_gpu, f_ref) <= ABS_TOL
+
+
+@pytest.mark.skipif(not orc.Reference.available(), reason="reference build (oracle/_ref) not present")
+def test_config_b16_seed0_against_reference(lib):
+    """The plain round trip at B = 16 exactly as the workload states it: coefficients re, im
+    U[-1, 1] from seed 0 (5,456 values); the GPU iDSOFT against the reference's IDSOFT, the GPU
+    DSOFT of that grid against the reference's DSOFT of the same grid, and the round trip within
+    the reference's own 1e-11 criterion (examples/example.cpp:44-74)."""
+    B = 16
+    c = orc.coeffs_uniform(B, seed=0)
+    assert c.size == 5456
+    ref = orc.Reference()
+    grid = gpu_idsoft(lib, c, B)
+    assert orc.rel_l2(grid, ref.idsoft(c, B, 1)) <= REL_TOL
+    f, _ = gpu_dsoft(lib, grid, B)
+    f_ref = ref.dsoft(grid, 1)
+    assert orc.rel_l2(f, f_ref) <= REL_TOL and orc.max_abs(f, f_ref) <= ABS_TOL
+    d = f - c
+    assert np.abs(d.real).max() <= 1e-11 and np.abs(d.imag).max() <= 1e-11
 
 
 def test_explicit_workspace_equals_library_workspace(lib):

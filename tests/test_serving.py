@@ -133,6 +133,60 @@ def test_same_alone_and_in_mix(lib):
 
 
 @pytest.mark.gpu
+def test_split_server_mixed_bandwidths(lib, oracle):
+    """Split mode: requests of one direction and different bandwidths share a batch and one
+    split-precision launch. Each result is bitwise the same alone and in the mix, within 1e-11
+    (relative L2) of the plain FP64 path, and the small ones match the long-double oracle."""
+    import torch
+
+    from oracle import oracle as orc
+    from pfsoftlib_b200.serving import TransformServer
+
+    tol = 1e-11
+    mix = _mix(lib, torch, n=24, seed=9)
+    with TransformServer(budget_bytes=2 << 30, max_batch=8, streams=3, split=True) as srv:
+        alone = []
+        for direction, B, inp, _ in mix:
+            o = _out_like(torch, direction, B)
+            srv.submit(direction, B, inp, o).wait()
+            alone.append(o)
+        srv.pause()
+        together, reqs = [], []
+        for direction, B, inp, _ in mix:
+            o = _out_like(torch, direction, B)
+            reqs.append(srv.submit(direction, B, inp, o))
+            together.append(o)
+        srv.resume()
+        for r in reqs:
+            r.wait()
+        st = srv.stats()
+        assert st["mean_batch"] > 2.0, st              # mixed bandwidths batched together
+        assert st["failed"] == 0
+    for (direction, B, inp, ref), a, t in zip(mix, alone, together):
+        assert torch.equal(a, t), f"B={B} dir={direction}: result differs alone vs in the mix"
+        assert _rel(a, ref) <= tol, f"B={B} dir={direction}: split served vs FP64 {_rel(a, ref):.2e}"
+        if B <= 16:
+            x = inp.cpu().numpy()
+            want = oracle.dsoft(x) if direction == 0 else oracle.idsoft(x, B)
+            assert orc.rel_l2(a.cpu().numpy().reshape(want.shape), want) <= tol, f"B={B} dir={direction} vs oracle"
+
+
+@pytest.mark.gpu
+def test_split_server_rejects_large_bandwidth(lib):
+    import torch
+
+    from pfsoftlib_b200 import _lib
+    from pfsoftlib_b200.serving import TransformServer
+
+    with TransformServer(budget_bytes=1 << 30, max_batch=4, streams=1, split=True) as srv:
+        c = torch.empty(257 * (4 * 257 * 257 - 1) // 3, dtype=torch.complex128, device="cuda")
+        g = torch.empty(514 ** 3, dtype=torch.complex128, device="cuda")
+        with pytest.raises(_lib.PfsoftError) as e:
+            srv.submit(1, 257, c, g)
+        assert e.value.status == _lib.PFSOFT_EINVAL
+
+
+@pytest.mark.gpu
 def test_continuous_admission_under_budget(lib):
     """Budget for 3 spectra at B=32: 40 requests arriving from another thread while batches run
     all finish, the arena never exceeds the budget, and batches overlap on the device."""
