@@ -125,10 +125,11 @@ def max_abs(x: np.ndarray, ref: np.ndarray) -> float:
 # ----------------------------------------------------------------------------- build
 
 def build(ref_root: str | None = None, quiet: bool = True) -> None:
-    """Build liboracle.so and, when the reference sources exist, _ref/libpfsoft_ref.so."""
+    """Build liboracle.so and, when a reference source tree is given (``ref_root``, else the
+    PFSOFT_REFERENCE environment variable) and present, _ref/libpfsoft_ref.so."""
     targets = ["oracle"]
-    ref_root = ref_root or "/root/reference"
-    if os.path.isdir(os.path.join(ref_root, "src")):
+    ref_root = ref_root or os.environ.get("PFSOFT_REFERENCE", "")
+    if ref_root and os.path.isdir(os.path.join(ref_root, "src")):
         targets.append("ref")
     cmd = ["make", "-s", "-C", HERE, f"REF={ref_root}"] + targets
     subprocess.run(cmd, check=True, stdout=subprocess.DEVNULL if quiet else None)

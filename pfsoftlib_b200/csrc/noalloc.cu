@@ -8,11 +8,14 @@
 // per-bandwidth tables, both allocated on first use; this entry point takes both from one
 // file-scope device array instead.
 //
-// Limit: bandwidth B <= 32 (a 64^3 complex128 spectrum, 4 MiB, plus 256 KiB for the tables).
-// Every GPU that loads the library holds this array until the process exits. All calls on a
-// device share it and it keeps the last call's contents; nothing in it has to start at zero
-// (the first FFT pass overwrites the whole spectrum before anything reads it, and the tables
-// are rebuilt whenever the bandwidth changes). Calls that overlap on the GPU race on it.
+// Limit: bandwidth B <= 32 (a 64^3 complex128 spectrum, 4 MiB, plus 320 KiB reserved for the
+// tables, of which B = 32 needs about 276 KiB). Every GPU that loads the library holds this
+// array until the process exits. All calls on a device share it and it keeps the last call's
+// contents; nothing in it has to start at zero (the first FFT pass overwrites the whole spectrum
+// before anything reads it, and the tables are rebuilt whenever the bandwidth changes). Calls
+// that overlap on the GPU race on it. Once a call has been recorded into a CUDA graph on a
+// device, every later call on that device rebuilds the tables (three small kernels): a graph
+// replay rewrites the array with its own bandwidth's tables, which the host cannot see.
 
 #include <cuda_runtime.h>
 
@@ -40,8 +43,9 @@ __device__ __align__(256) unsigned char g_noalloc_scratch[kSpectrumBytes + kTabl
 
 struct NoAllocDevice {
     bool ready;          // symbol address resolved on this device
+    bool captured;       // a call was recorded into a graph: the host no longer knows the tables
     unsigned char* base; // device address of g_noalloc_scratch
-    int tables_B;        // bandwidth whose tables the array holds (0 = none)
+    int tables_B;        // bandwidth whose tables the array holds (0 = unknown)
     BandTables tables;
 };
 
@@ -79,13 +83,18 @@ int pfsoft_cuda_dsoft_noalloc(const double* d_grid, int B, double* d_coeffs, voi
         d.ready = true;
         d.tables_B = 0;
     }
-    if (d.tables_B != B) {
+    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+    if (cudaStreamIsCapturing(s, &cap) != cudaSuccess)
+        return fail(PFSOFT_ECUDA, "pfsoft_cuda_dsoft_noalloc: cudaStreamIsCapturing failed");
+    if (cap != cudaStreamCaptureStatusNone) d.captured = true;
+    if (d.captured || d.tables_B != B) {
+        // recorded into the captured work too, so that every replay builds the tables it reads
         if (tables_bytes(B) > kTableBytes) return fail(PFSOFT_EINVAL, "pfsoft_cuda_dsoft_noalloc: tables exceed the reserve");
         if (tables_build(B, d.base + kSpectrumBytes, &d.tables, s) != cudaSuccess) {
             d.tables_B = 0;
             return fail(PFSOFT_ECUDA, "pfsoft_cuda_dsoft_noalloc: table kernels failed to launch");
         }
-        d.tables_B = B;
+        d.tables_B = d.captured ? 0 : B;
     }
     const BandTables& t = d.tables;
     const int N = 2 * B;
@@ -98,7 +107,7 @@ int pfsoft_cuda_dsoft_noalloc(const double* d_grid, int B, double* d_coeffs, voi
     memset(&f, 0, sizeof(f));
     f.n = N;
     f.nvec = N;
-    f.kb = 8;
+    f.kb = fft_tile_vectors(N);
     f.nstages = fft_plan_radices(N, f.radix, f.ns);
     f.scale = 1.0;
     f.twiddle = t.twiddle;

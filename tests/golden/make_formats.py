@@ -1,6 +1,7 @@
 """Writes tests/golden/formats_ref.txt: the output of tests/cpp/formats.cpp compiled against the
 reference's own headers and sources (the compiled reference in oracle/_ref, built by
-oracle/Makefile). Run here, where the reference is present:  python tests/golden/make_formats.py
+oracle/Makefile). Run where the reference source tree is present:
+    PFSOFT_REFERENCE=<reference source tree> python tests/golden/make_formats.py
 """
 import os
 import subprocess
@@ -9,11 +10,13 @@ import tempfile
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(os.path.dirname(HERE))
-REF = os.environ.get("PFSOFT_REFERENCE", "/root/reference")
+REF = os.environ.get("PFSOFT_REFERENCE", "")
 
 
 def main() -> int:
-    subprocess.run(["make", "-C", os.path.join(ROOT, "oracle"), "ref"], check=True, capture_output=True)
+    if not REF:
+        sys.exit("set PFSOFT_REFERENCE to the reference project's source tree")
+    subprocess.run(["make", "-C", os.path.join(ROOT, "oracle"), f"REF={REF}", "ref"], check=True, capture_output=True)
     with tempfile.TemporaryDirectory() as tmp:
         exe = os.path.join(tmp, "formats_ref")
         subprocess.run(["/usr/bin/g++", "-std=c++11", "-O1", "-w", "-fopenmp", "-DUSE_REFERENCE",

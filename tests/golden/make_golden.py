@@ -31,7 +31,7 @@ PAIRS = [(0, 0), (1, 0), (1, 1), (2, -1), (-3, 2), (3, 3)]
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--ref", default="/root/reference")
+    ap.add_argument("--ref", required=True, help="the reference project's source tree")
     a = ap.parse_args()
     orc.build(a.ref)
     ref = orc.Reference()

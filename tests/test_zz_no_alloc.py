@@ -48,6 +48,39 @@ def test_noalloc_matches_dsoft_on_two_calls_in_a_row(lib):
         assert orc.max_abs(got, ref) <= ABS_TOL
 
 
+def test_noalloc_bandwidth_sequence(lib):
+    """Each call changes the bandwidth (small and odd FFT lengths: generic and direct-radix plans,
+    a leading radix-1 stage; tables rebuilt from smaller to larger and back)."""
+    for i, B in enumerate((1, 3, 5, 31, 32, 8)):
+        grid = _grid(B, 40 + i)
+        got = _dsoft(lib, "noalloc", grid, B)
+        ref = _dsoft(lib, "dsoft", grid, B)
+        assert orc.rel_l2(got, ref) <= REL_TOL, B
+        assert orc.max_abs(got, ref) <= ABS_TOL, B
+
+
+def test_noalloc_graph_replay_then_eager(lib):
+    """A call captured into a CUDA graph at B = 32, an eager call at B = 16, the graph replayed,
+    then another eager call at B = 16: every result matches pfsoft_cuda_dsoft (the replay rewrites
+    the shared tables, so later calls rebuild theirs)."""
+    g32, g16 = _grid(32, 5), _grid(16, 6)
+    ref32, ref16 = _dsoft(lib, "dsoft", g32, 32), _dsoft(lib, "dsoft", g16, 16)
+    d32 = torch.from_numpy(g32).cuda()
+    o32 = torch.empty(orc.coef_count(32), dtype=torch.complex128, device="cuda")
+    _dsoft(lib, "noalloc", g32, 32)   # first call on the device: symbol address, outside the capture
+    side = torch.cuda.Stream()
+    graph = torch.cuda.CUDAGraph()
+    with torch.cuda.stream(side):
+        with torch.cuda.graph(graph, stream=side):
+            assert lib.pfsoft_cuda_dsoft_noalloc(d32.data_ptr(), 32, o32.data_ptr(), side.cuda_stream) == 0
+    assert orc.rel_l2(_dsoft(lib, "noalloc", g16, 16), ref16) <= REL_TOL
+    o32.fill_(complex(np.nan, np.nan))
+    graph.replay()
+    torch.cuda.synchronize()
+    assert orc.rel_l2(o32.cpu().numpy(), ref32) <= REL_TOL
+    assert orc.rel_l2(_dsoft(lib, "noalloc", g16, 16), ref16) <= REL_TOL
+
+
 def test_noalloc_repeat_same_bandwidth(lib):
     grid = _grid(32, 3)
     a = _dsoft(lib, "noalloc", grid, 32)
