@@ -149,6 +149,8 @@ class Oracle:
         lib.oracle_quadrature_weights.argtypes = [ctypes.c_int, _dp]
         lib.oracle_wigner_d.argtypes = [ctypes.c_int] * 4 + [_dp]
         lib.oracle_fft2_layers.argtypes = [ctypes.c_int, ctypes.c_int, _dp, _dp, ctypes.c_int]
+        lib.oracle_dwt_forward.argtypes = [_dp, ctypes.c_int, ctypes.c_void_p, ctypes.c_int, _dp]
+        lib.oracle_dwt_inverse.argtypes = [_dp, ctypes.c_int, ctypes.c_void_p, ctypes.c_int, _dp]
         self.lib = lib
 
     def dsoft(self, grid: np.ndarray) -> np.ndarray:
@@ -164,6 +166,27 @@ class Oracle:
         N = 2 * B
         out = np.empty((N, N, N), dtype=np.complex128)
         self.lib.oracle_idsoft(_ptr(c.view(np.float64)), B, _ptr(out.view(np.float64)))
+        return out
+
+    def dwt_forward(self, spectrum: np.ndarray, B: int, classes=None, out: np.ndarray | None = None) -> np.ndarray:
+        """The DWT stage on the bin-major spectrum X[row][col][k] for `classes` (None: all),
+        writing only their coefficients into `out` (zeros when not given)."""
+        x = np.ascontiguousarray(spectrum, dtype=np.complex128).reshape(-1)
+        out = np.zeros(coef_count(B), dtype=np.complex128) if out is None else out
+        cl = None if classes is None else np.ascontiguousarray(classes, dtype=np.int32)
+        self.lib.oracle_dwt_forward(_ptr(x.view(np.float64)), B, None if cl is None else cl.ctypes.data,
+                                    -1 if cl is None else len(cl), _ptr(out.view(np.float64)))
+        return out
+
+    def dwt_inverse(self, coeffs: np.ndarray, B: int, classes=None, out: np.ndarray | None = None) -> np.ndarray:
+        """The inverse DWT stage into the bin-major spectrum `out` (zeros when not given), writing
+        only the beta columns of the bins of `classes` (None: all)."""
+        c = np.ascontiguousarray(coeffs, dtype=np.complex128)
+        N = 2 * B
+        out = np.zeros(N ** 3, dtype=np.complex128) if out is None else out
+        cl = None if classes is None else np.ascontiguousarray(classes, dtype=np.int32)
+        self.lib.oracle_dwt_inverse(_ptr(c.view(np.float64)), B, None if cl is None else cl.ctypes.data,
+                                    -1 if cl is None else len(cl), _ptr(out.view(np.float64)))
         return out
 
     def weights(self, B: int) -> np.ndarray:

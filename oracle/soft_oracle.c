@@ -369,3 +369,88 @@ void oracle_idsoft(const double* coeffs, int B, double* grid)
     }
     free(H);
 }
+
+/* The discrete Wigner transform stage alone (fn_dsoft.cpp:134-283 / fn_idsoft.cpp:124-283), on
+ * the engine's bin-major spectrum X[row][col][k] (the unnormalised layer-wise 2D DFT with beta
+ * innermost), for a list of order classes only (indices in the M-major enumeration; NULL with
+ * n < 0 = every class). Test infrastructure for the sharded transform, whose ranks each run the
+ * DWT of their own classes. Forward: writes the classes' coefficients, scaled pi/(2B^2); every
+ * other coefficient is left as it is. Inverse: writes the beta columns of the classes' bins,
+ * scaled 2B^2/pi; every other value of X is left as it is. */
+static void class_orders_ld(int c, int* M, int* Mp)
+{
+    int m = (int)((sqrt(8.0 * c + 1.0) - 1.0) / 2.0);
+    while (m * (m + 1) / 2 > c) --m;
+    while ((m + 1) * (m + 2) / 2 <= c) ++m;
+    *M = m;
+    *Mp = c - m * (m + 1) / 2;
+}
+
+void oracle_dwt_forward(const double* X, int B, const int* classes, int n, double* coeffs)
+{
+    const int N = 2 * B;
+    const int count = n < 0 ? B * (B + 1) / 2 : n;
+    ld* w = (ld*)malloc(sizeof(ld) * N);
+    oracle_quadrature_weights_ld(B, w);
+    const ld norm = PI_L / ((ld)B * N);
+    ld* d = (ld*)malloc(sizeof(ld) * (size_t)B * N);
+    for (int i = 0; i < count; ++i) {
+        int M, Mp;
+        class_orders_ld(n < 0 ? i : classes[i], &M, &Mp);
+        oracle_wigner_d_ld(B, M, Mp, w, d);
+        int m1s[8], m2s[8];
+        const int nc = class_cases(M, Mp, m1s, m2s);
+        for (int q = 0; q < nc; ++q) {
+            const int m1 = m1s[q], m2 = m2s[q];
+            const int row = ((m2 % N) + N) % N, col = ((m1 % N) + N) % N;
+            const int rev = case_rev(m1, m2);
+            const double* s = X + 2 * ((size_t)row * N + col) * N;
+            for (int l = M; l < B; ++l) {
+                const ld* dl = d + (size_t)(l - M) * N;
+                ldc acc = 0;
+                for (int k = 0; k < N; ++k) acc += dl[rev ? N - 1 - k : k] * (s[2 * k] + I * (ld)s[2 * k + 1]);
+                acc *= norm * case_sign(m1, m2, l);
+                const size_t o = oracle_coef_index(l, m1, m2);
+                coeffs[2 * o] = (double)creall(acc);
+                coeffs[2 * o + 1] = (double)cimagl(acc);
+            }
+        }
+    }
+    free(d);
+    free(w);
+}
+
+void oracle_dwt_inverse(const double* coeffs, int B, const int* classes, int n, double* X)
+{
+    const int N = 2 * B;
+    const int count = n < 0 ? B * (B + 1) / 2 : n;
+    const ld norm = (ld)B * N / PI_L;
+    ld* d = (ld*)malloc(sizeof(ld) * (size_t)B * N);
+    ldc* g = (ldc*)malloc(sizeof(ldc) * B);
+    for (int i = 0; i < count; ++i) {
+        int M, Mp;
+        class_orders_ld(n < 0 ? i : classes[i], &M, &Mp);
+        oracle_wigner_d_ld(B, M, Mp, NULL, d);
+        int m1s[8], m2s[8];
+        const int nc = class_cases(M, Mp, m1s, m2s);
+        for (int q = 0; q < nc; ++q) {
+            const int m1 = m1s[q], m2 = m2s[q];
+            const int row = ((m2 % N) + N) % N, col = ((m1 % N) + N) % N;
+            const int rev = case_rev(m1, m2);
+            for (int l = M; l < B; ++l) {
+                const size_t o = oracle_coef_index(l, m1, m2);
+                g[l - M] = norm * case_sign(m1, m2, l) * (coeffs[2 * o] + I * (ld)coeffs[2 * o + 1]);
+            }
+            double* s = X + 2 * ((size_t)row * N + col) * N;
+            for (int k = 0; k < N; ++k) {
+                const int kk = rev ? N - 1 - k : k;
+                ldc acc = 0;
+                for (int l = M; l < B; ++l) acc += d[(size_t)(l - M) * N + kk] * g[l - M];
+                s[2 * k] = (double)creall(acc);
+                s[2 * k + 1] = (double)cimagl(acc);
+            }
+        }
+    }
+    free(g);
+    free(d);
+}

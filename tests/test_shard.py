@@ -74,17 +74,24 @@ def test_host_queries(lib):
 # ---- gloo: the orchestration with CPU steps ----------------------------------------------------
 
 class CpuSteps:
-    """ShardPlan's step interface on CPU tensors. The DWT is replaced by copying the owned bins'
-    beta columns, so the 'coefficients' are the (N^3) spectrum itself; the exchange uses the
-    plan's copy runs."""
+    """ShardPlan's step interface on CPU tensors; the exchange uses the plan's copy runs. With
+    real=False the DWT is replaced by copying the owned bins' beta columns (the 'coefficients' are
+    the (N^3) spectrum itself); with real=True each rank runs the long-double oracle's DWT stage
+    on its own order classes (oracle/soft_oracle.c: oracle_dwt_forward / oracle_dwt_inverse)."""
 
-    def __init__(self, B, nranks, rank):
+    def __init__(self, B, nranks, rank, real=False):
         from pfsoftlib_b200.shard import ShardPlan
 
         self.p = ShardPlan(B, nranks, rank)
         self.B, self.N, self.nranks, self.rank = B, 2 * B, nranks, rank
         self.own = self.p.bins(rank)
         self.run = {(d, s): self.p.runs(d, s) for d in (0, 1) for s in (0, 1, 2)}
+        self.real = real
+        if real:
+            from oracle.oracle import Oracle
+
+            self.oracle = Oracle()
+            self.cls = self.p.classes(rank)
 
     layers = property(lambda self: self.p.layers)
 
@@ -98,7 +105,7 @@ class CpuSteps:
         return self.N ** 3
 
     def coef_elems(self):
-        return self.N ** 3
+        return self.B * (4 * self.B * self.B - 1) // 3 if self.real else self.N ** 3
 
     def _copy(self, d, step, src, dst):
         r = self.run[(d, step)]
@@ -128,12 +135,20 @@ class CpuSteps:
 
     def dwt_forward(self, spec, coeffs):
         N = self.N
+        if self.real:
+            c = coeffs.numpy()
+            c[:] = 0
+            self.oracle.dwt_forward(spec.numpy(), self.B, self.cls, out=c)
+            return
         c = coeffs.numpy().reshape(N * N, N)
         c[:] = 0
         c[self.own] = spec.numpy().reshape(N * N, N)[self.own]
 
     def dwt_inverse(self, coeffs, spec):
         N = self.N
+        if self.real:
+            self.oracle.dwt_inverse(coeffs.numpy(), self.B, self.cls, out=spec.numpy())
+            return
         spec.numpy().reshape(N * N, N)[self.own] = coeffs.numpy().reshape(N * N, N)[self.own]
 
 
@@ -184,8 +199,38 @@ def _gloo_rank(rank, world, port, B, errq):
         raise
 
 
-@pytest.mark.parametrize("world,B", [(2, 8), (3, 5)])
-def test_sharded_transform_gloo(world, B):
+def _gloo_rank_oracle(rank, world, port, B, errq):
+    """Each rank runs the oracle's DWT on its own classes: the assembled coefficients (all-reduce)
+    against the oracle's DSOFT of the whole grid, and each rank's inverse slab against the
+    oracle's IDSOFT, both within 1e-13 relative L2."""
+    import torch
+    import torch.distributed as dist
+
+    from oracle import oracle as orc
+    from pfsoftlib_b200.shard import ShardedTransform
+
+    try:
+        os.environ["MASTER_ADDR"], os.environ["MASTER_PORT"] = "127.0.0.1", str(port)
+        dist.init_process_group("gloo", rank=rank, world_size=world)
+        ora = orc.Oracle()
+        c = orc.coeffs_uniform(B, seed=31)
+        grid = ora.idsoft(c, B)
+        st = ShardedTransform(B, device="cpu", engine=CpuSteps(B, world, rank, real=True))
+        first, count = st.layers
+        f = st.dsoft(torch.from_numpy(grid[first:first + count].copy()))
+        assert orc.rel_l2(f.numpy(), ora.dsoft(grid)) <= 1e-13, "forward vs oracle"
+        assert orc.rel_l2(f.numpy(), c) <= 1e-13, "round trip"
+        slab = st.idsoft(torch.from_numpy(c.copy()))
+        assert orc.rel_l2(slab.numpy().reshape(count, 2 * B, 2 * B), grid[first:first + count]) <= 1e-13, "inverse"
+        dist.barrier()
+        dist.destroy_process_group()
+    except BaseException as e:   # reported to the parent
+        errq.put(f"rank {rank}: {type(e).__name__}: {e}")
+        raise
+
+
+@pytest.mark.parametrize("world,B,target", [(2, 8, "copy"), (3, 5, "copy"), (2, 6, "oracle"), (3, 7, "oracle")])
+def test_sharded_transform_gloo(world, B, target):
     import torch.multiprocessing as mp
 
     from pfsoftlib_b200 import _lib
@@ -196,7 +241,8 @@ def test_sharded_transform_gloo(world, B):
         port = s.getsockname()[1]
     ctx = mp.get_context("spawn")
     errq = ctx.Queue()
-    procs = [ctx.Process(target=_gloo_rank, args=(r, world, port, B, errq)) for r in range(world)]
+    fn = _gloo_rank if target == "copy" else _gloo_rank_oracle
+    procs = [ctx.Process(target=fn, args=(r, world, port, B, errq)) for r in range(world)]
     for p in procs:
         p.start()
     for p in procs:
