@@ -49,7 +49,7 @@ int pfsoft_version(void);
 /* Sizes. */
 size_t pfsoft_coef_count(int B);            /* B(4B^2-1)/3 complex values */
 size_t pfsoft_grid_bytes(int B);            /* (2B)^3 * 16 */
-size_t pfsoft_workspace_bytes(int B);       /* device scratch for one transform */
+size_t pfsoft_workspace_bytes(int B);       /* device scratch for one transform: (2B)^3 * 16 + 4096 */
 
 /* ---- Forward / inverse transforms on device-resident data (stream ordered) -------------
  * pfsoft_cuda_dsoft replaces pfsoft::FourierTransforms::DSOFT
@@ -276,6 +276,10 @@ long long pfsoft_launch_count(void);
 /* Tuning knob used by the autotuner: direction 0 = DSOFT, 1 = IDSOFT; case_split 1 = each warp
  * applies all eight symmetry cases, 2 = warp pairs split them, 0 = library default. */
 int pfsoft_tune_dwt_case_split(int direction, int case_split);
+/* Tuning knob: on != 0 (the default) runs the two FFT passes of a direction in one persistent
+ * launch, layer chunk by layer chunk, so that the second pass reads the first pass's output from
+ * L2; 0 runs them as two launches. Process-wide; for measurements and the autotuner. */
+int pfsoft_tune_fft_fused(int on);
 /* Test knob for the split-precision DWT's failure path (no counterpart in the reference): when
  * wait_ns > 0, every later split launch first waits up to wait_ns nanoseconds on a barrier that
  * nothing signals, before it issues any MMA; the wait runs out, every warp of the kernel leaves,

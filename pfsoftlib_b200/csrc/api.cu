@@ -104,9 +104,10 @@ DeviceState* device_state(int dev)
 
 // ---- launch accounting and optional per-stage timing ------------------------------------
 enum Stage { ST_FFT_FWD_ROWS, ST_FFT_FWD_COLS, ST_DWT_FWD, ST_NYQUIST, ST_DWT_INV, ST_FFT_INV_COLS, ST_FFT_INV_ROWS,
-             ST_TABLES, ST_COUNT };
+             ST_TABLES, ST_FFT_FWD_FUSED, ST_FFT_INV_FUSED, ST_COUNT };
 const char* kStageNames[ST_COUNT] = {"fft_forward_gamma", "fft_forward_alpha", "dwt_forward", "zero_nyquist",
-                                     "dwt_inverse", "fft_inverse_alpha", "fft_inverse_gamma", "tables"};
+                                     "dwt_inverse", "fft_inverse_alpha", "fft_inverse_gamma", "tables",
+                                     "fft_forward_fused", "fft_inverse_fused"};
 
 std::atomic<long long> g_launches{0};
 
@@ -246,7 +247,7 @@ int check_transform_args(const void* a, const void* b, int B, void*& ws, size_t 
 {
     if (!valid_bandwidth(B)) return fail(PFSOFT_EINVAL, "bandwidth must be in [1, 512]");
     if (!a || !b) return fail(PFSOFT_EINVAL, "null data pointer");
-    const size_t need = grid_elems(B) * sizeof(double2);
+    const size_t need = grid_elems(B) * sizeof(double2) + kFftSyncBytes;
     if (ws) {
         if (ws_bytes < need) return fail(PFSOFT_EINVAL, "workspace smaller than pfsoft_workspace_bytes(B)");
         if ((reinterpret_cast<uintptr_t>(ws) & 15) != 0) return fail(PFSOFT_EINVAL, "workspace not 16-byte aligned");
@@ -269,13 +270,19 @@ int run_dsoft(const double* d_grid, int B, double* d_coeffs, void* ws, cudaStrea
     // F2: vectors = layers k, tile = gamma bin r, elements = column c; in place on X
     FftPassArgs f2 = pass_args(N, N, t, FftStrides{1, n2, n}, FftStrides{1, n2, n}, 1.0);
     if (f1.nstages == 0) return fail(PFSOFT_EINVAL, "FFT length cannot be planned");
-    {
-        StageScope sc(ST_FFT_FWD_ROWS, s);
-        PF_CUDA(fft_pass_launch(G, X, f1, N, -1, s));
-    }
-    {
-        StageScope sc(ST_FFT_FWD_COLS, s);
-        PF_CUDA(fft_pass_launch(X, X, f2, N, -1, s));
+    if (fft_fused_enabled() && fft_fused_chunk(f1, f2)) {
+        // both passes in one launch; the counters sit past the spectrum in the workspace
+        StageScope sc(ST_FFT_FWD_FUSED, s);
+        PF_CUDA(fft_fused_launch(-1, f1, f2, N, N, 1, G, X, X, X, X, (long long)grid_elems(B), s));
+    } else {
+        {
+            StageScope sc(ST_FFT_FWD_ROWS, s);
+            PF_CUDA(fft_pass_launch(G, X, f1, N, -1, s));
+        }
+        {
+            StageScope sc(ST_FFT_FWD_COLS, s);
+            PF_CUDA(fft_pass_launch(X, X, f2, N, -1, s));
+        }
     }
     DwtArgs a = dwt_args(t);
     {
@@ -308,13 +315,18 @@ int run_idsoft(const double* d_coeffs, int B, double* d_grid, void* ws, cudaStre
     // I1: inverse DFT over gamma, X[r][c][k] -> G[k][c][r], scaled by 1/(4B^2) (src/fn_idsoft.cpp:289)
     FftPassArgs i1 = pass_args(N, N, t, FftStrides{1, n, n2}, FftStrides{n2, n, 1}, 1.0 / (4.0 * B * B));
     if (i1.nstages == 0) return fail(PFSOFT_EINVAL, "FFT length cannot be planned");
-    {
-        StageScope sc(ST_FFT_INV_COLS, s);
-        PF_CUDA(fft_pass_launch(X, X, i2, N, +1, s));
-    }
-    {
-        StageScope sc(ST_FFT_INV_ROWS, s);
-        PF_CUDA(fft_pass_launch(X, G, i1, N, +1, s));
+    if (fft_fused_enabled() && fft_fused_chunk(i2, i1)) {
+        StageScope sc(ST_FFT_INV_FUSED, s);
+        PF_CUDA(fft_fused_launch(+1, i2, i1, N, N, 1, X, X, X, G, X, (long long)grid_elems(B), s));
+    } else {
+        {
+            StageScope sc(ST_FFT_INV_COLS, s);
+            PF_CUDA(fft_pass_launch(X, X, i2, N, +1, s));
+        }
+        {
+            StageScope sc(ST_FFT_INV_ROWS, s);
+            PF_CUDA(fft_pass_launch(X, G, i1, N, +1, s));
+        }
     }
     return PFSOFT_OK;
 }
@@ -434,7 +446,7 @@ size_t pfsoft_coef_count(int B) { return B < 1 ? 0 : coef_offset(B); }
 
 size_t pfsoft_grid_bytes(int B) { return B < 1 ? 0 : grid_elems(B) * sizeof(double2); }
 
-size_t pfsoft_workspace_bytes(int B) { return B < 1 ? 0 : grid_elems(B) * sizeof(double2); }
+size_t pfsoft_workspace_bytes(int B) { return B < 1 ? 0 : grid_elems(B) * sizeof(double2) + kFftSyncBytes; }
 
 int pfsoft_cuda_dsoft(const double* d_grid, int B, double* d_coeffs, void* d_workspace, size_t workspace_bytes,
                       void* stream)
@@ -477,7 +489,7 @@ static int host_staged(int B, bool forward, const double* in, double* out)
     };
     cudaError_t e = grow(&st->h_grid, &st->h_grid_bytes, gb);
     if (e == cudaSuccess) e = grow(&st->h_coef, &st->h_coef_bytes, cb);
-    if (e == cudaSuccess) e = grow(&st->h_ws, &st->h_ws_bytes, gb);
+    if (e == cudaSuccess) e = grow(&st->h_ws, &st->h_ws_bytes, gb + kFftSyncBytes);
     if (e != cudaSuccess) return fail(PFSOFT_ENOMEM, std::string("staging allocation: ") + cudaGetErrorString(e));
     cudaStream_t s = st->h_stream;
     int rc;
@@ -648,6 +660,12 @@ int pfsoft_cuda_wigner_d_matrix(int B, int M, int Mp, int weighted, double* d_ou
 }
 
 long long pfsoft_launch_count(void) { return g_launches.load(); }
+
+int pfsoft_tune_fft_fused(int on)
+{
+    fft_set_fused(on != 0);
+    return PFSOFT_OK;
+}
 
 int pfsoft_tune_dwt_case_split(int direction, int case_split)
 {

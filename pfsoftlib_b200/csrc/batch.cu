@@ -134,6 +134,15 @@ int launch_group(int dir, const BandTables& t, int T, double2** d_grids, double2
     auto pass = [&](bool first) {
         return fft_pass_launch(nullptr, nullptr, group_pass_args(dir, first, t, d_grids, d_ws), t.N, sign, s, T);
     };
+    // both passes of the direction: one fused launch (counters past each spectrum) or two
+    auto passes = [&]() -> cudaError_t {
+        const FftPassArgs a = group_pass_args(dir, true, t, d_grids, d_ws), b = group_pass_args(dir, false, t, d_grids, d_ws);
+        if (fft_fused_enabled() && fft_fused_chunk(a, b))
+            return fft_fused_launch(sign, a, b, t.N, t.N, T, nullptr, nullptr, nullptr, nullptr, nullptr,
+                                    (long long)t.N * t.N * t.N, s);
+        cudaError_t e = pass(true);
+        return e == cudaSuccess ? pass(false) : e;
+    };
     auto dwt = [&]() -> cudaError_t {
         if (t.B > kBatchMaxFused) return dwt_per_transform(dir, t, T, h_ws, h_coef, s);
         cudaError_t e = cudaMemsetAsync(d_counter, 0, sizeof(int), s);
@@ -142,14 +151,12 @@ int launch_group(int dir, const BandTables& t, int T, double2** d_grids, double2
     };
     cudaError_t e;
     if (dir == 0) {
-        e = pass(true);
-        if (e == cudaSuccess) e = pass(false);
+        e = passes();
         if (e == cudaSuccess) e = dwt();
     } else {
         e = zero_nyquist_launch(d_ws, t.B, T, s);
         if (e == cudaSuccess) e = dwt();
-        if (e == cudaSuccess) e = pass(true);
-        if (e == cudaSuccess) e = pass(false);
+        if (e == cudaSuccess) e = passes();
     }
     if (e != cudaSuccess) return fail(PFSOFT_ECUDA, std::string("group launch: ") + cudaGetErrorString(e));
     return PFSOFT_OK;
@@ -229,6 +236,16 @@ int enqueue(pfsoft_batch* b, int dir, cudaStream_t s)
         FftPassArgs a = group_pass_args(dir, first_pass, g.tables, b->grid_ptrs() + g.ptr_base, b->ws_ptrs() + g.ptr_base);
         return fft_pass_launch(nullptr, nullptr, a, g.N, sign, s, (int)g.members.size());
     };
+    // both passes of a group: one fused launch when the plan allows, else the two passes
+    auto fft_both = [&](const pfsoft_batch::Group& g) -> cudaError_t {
+        const FftPassArgs a = group_pass_args(dir, true, g.tables, b->grid_ptrs() + g.ptr_base, b->ws_ptrs() + g.ptr_base);
+        const FftPassArgs c = group_pass_args(dir, false, g.tables, b->grid_ptrs() + g.ptr_base, b->ws_ptrs() + g.ptr_base);
+        if (fft_fused_enabled() && fft_fused_chunk(a, c))
+            return fft_fused_launch(sign, a, c, g.N, g.N, (int)g.members.size(), nullptr, nullptr, nullptr, nullptr, nullptr,
+                                    (long long)g.N * g.N * g.N + (g.split ? (long long)dwt_split_aux_elems(g.B) : 0), s);
+        cudaError_t e = fft_group(g, true);
+        return e == cudaSuccess ? fft_group(g, false) : e;
+    };
     auto dwt_large = [&](const pfsoft_batch::Group& g) -> cudaError_t {
         const size_t c = (size_t)b->count;
         return dwt_per_transform(dir, g.tables, (int)g.members.size(), b->h_ptr + 2 * c + g.ptr_base,
@@ -237,9 +254,7 @@ int enqueue(pfsoft_batch* b, int dir, cudaStream_t s)
     cudaError_t e = cudaSuccess;
     if (dir == 0) {
         for (const auto& g : b->groups)
-            if (e == cudaSuccess) e = fft_group(g, true);
-        for (const auto& g : b->groups)
-            if (e == cudaSuccess) e = fft_group(g, false);
+            if (e == cudaSuccess) e = fft_both(g);
         if (e == cudaSuccess && b->n_items > 0) {
             e = cudaMemsetAsync(b->d_counter, 0, sizeof(int), s);
             if (e == cudaSuccess) e = dwt_batch_launch(0, b->d_groups_fwd, b->d_items, b->n_items, b->d_counter, b->tpc, b->nmax, s);
@@ -272,9 +287,7 @@ int enqueue(pfsoft_batch* b, int dir, cudaStream_t s)
         for (const auto& g : b->groups)
             if (e == cudaSuccess && g.B > kBatchMaxFused && !g.split) e = dwt_large(g);
         for (const auto& g : b->groups)
-            if (e == cudaSuccess) e = fft_group(g, true);
-        for (const auto& g : b->groups)
-            if (e == cudaSuccess) e = fft_group(g, false);
+            if (e == cudaSuccess) e = fft_both(g);
     }
     if (e != cudaSuccess) return fail(PFSOFT_ECUDA, std::string("batch launch: ") + cudaGetErrorString(e));
     return PFSOFT_OK;
@@ -329,7 +342,7 @@ int pfsoft_batch_create(const int* bandwidths, int count, int transforms_per_cta
         g.split = (flags & PFSOFT_BATCH_SPLIT) && dwt_split_supported(g.B);
         for (int t : g.members) {
             ws_off[t] = ws_total;
-            ws_total += ((size_t)g.N * g.N * g.N + (g.split ? dwt_split_aux_elems(g.B) : 0)) * sizeof(double2);
+            ws_total += ((size_t)g.N * g.N * g.N + (g.split ? dwt_split_aux_elems(g.B) : 0)) * sizeof(double2) + kFftSyncBytes;
         }
         int rc = tables_for(g.B, nullptr, &g.tables);
         if (rc) {

@@ -15,6 +15,9 @@
 // contiguous (sv == 1), so KB*16 bytes move per group of KB lanes. That is how the beta <->
 // (alpha, gamma) transpose rides inside the first and last stage at no extra HBM traffic.
 
+#include <algorithm>
+#include <cstring>
+
 #include "common.cuh"
 #include "fft.cuh"
 
@@ -136,6 +139,14 @@ __device__ __forceinline__ double2 twiddle(const double2* __restrict__ tw, int t
     return sign < 0 ? w : make_double2(w.x, -w.y);
 }
 
+// First-stage load of a pass: the read-only path, unless the pass reads what another CTA of the
+// same launch wrote (the second pass of fft_fused_kernel), which needs coherent loads.
+__device__ __forceinline__ double2 load_src(const FftPassArgs& a, const double2* p)
+{
+    if (a.coherent) return __ldcg(p);   // L2, where the other CTAs' stores are
+    return __ldg(p);
+}
+
 // smem position of element i of a vector (one pad slot every 16 elements)
 __device__ __forceinline__ int spos(int i) { return i + (i >> 4); }
 
@@ -169,7 +180,7 @@ __device__ __forceinline__ void run_stage_fixed(const FftPassArgs& a, int s, con
         if (first) {
             const double2* p = gsrc + src_base + (long long)kk * a.src.sv;
 #pragma unroll
-            for (int r = 0; r < R; ++r) v[r] = __ldg(p + (long long)(j + r * m) * a.src.se);
+            for (int r = 0; r < R; ++r) v[r] = load_src(a, p + (long long)(j + r * m) * a.src.se);
         } else {
             const double2* p = sin_ + kk * pl;
 #pragma unroll
@@ -234,7 +245,7 @@ __device__ __forceinline__ void run_stage_inplace(const FftPassArgs& a, int s, c
             if (first) {
                 const double2* q = gsrc + src_base + (long long)kk[p] * a.src.sv;
 #pragma unroll
-                for (int r = 0; r < R; ++r) v[p][r] = __ldg(q + (long long)(j[p] + r * m) * a.src.se);
+                for (int r = 0; r < R; ++r) v[p][r] = load_src(a, q + (long long)(j[p] + r * m) * a.src.se);
             } else {
                 const double2* q = buf + kk[p] * pl;
 #pragma unroll
@@ -277,18 +288,24 @@ __device__ __forceinline__ void run_stage_inplace(const FftPassArgs& a, int s, c
 // 529-560 us (623-650), n = 192 50-54 us (84-90), n = 96 12.6 us (18.7-19.0), n = 32 6.6 us
 // (8.1-8.7); at n = 512, 8-vector tiles with two 16-warp CTAs per SM came within 2 %.
 template <int SIGN, int R0, int R1, int R2, int R3, int P0, int P1, int P2, int P3>
-__global__ void __launch_bounds__(256, 4) fft_pass_inplace_kernel(const double2* src, double2* dst,
-                                                                  const FftPassArgs a)
+struct InplaceTile {
+    // CTAs per SM of the fused kernel (fft_fused_kernel): its item loop and both passes' arguments
+    // do not fit the stand-alone kernel's 64 registers
+    static constexpr int kMinBlocks = 2;
+    // tile (bx, by) of a pass: vectors bx*kb .., tile index by
+    static __device__ __forceinline__ void run(const FftPassArgs& a, int bx, int by, const double2* src, double2* dst,
+                                               double2* smem);
+};
+
+template <int SIGN, int R0, int R1, int R2, int R3, int P0, int P1, int P2, int P3>
+__device__ __forceinline__ void InplaceTile<SIGN, R0, R1, R2, R3, P0, P1, P2, P3>::run(const FftPassArgs& a, int bx, int by,
+                                                                                    const double2* src, double2* dst,
+                                                                                    double2* smem)
 {
-    extern __shared__ double2 smem[];
-    if (a.srcs) {
-        src = a.srcs[blockIdx.z];
-        dst = a.dsts[blockIdx.z];
-    }
-    const int v0 = blockIdx.x * a.kb;
+    const int v0 = bx * a.kb;
     const int nv = min(a.kb, a.nvec - v0);
-    const long long src_base = (long long)v0 * a.src.sv + (long long)blockIdx.y * a.src.sb;
-    const long long dst_base = (long long)v0 * a.dst.sv + (long long)blockIdx.y * a.dst.sb;
+    const long long src_base = (long long)v0 * a.src.sv + (long long)by * a.src.sb;
+    const long long dst_base = (long long)v0 * a.dst.sv + (long long)by * a.dst.sb;
     if constexpr (R0 == R1 && R1 == R2 && R3 == 0 && P0 == P1 && P1 == P2) {
         // one radix throughout (n = 512): a loop over the runtime stage count, which compiles
         // to fewer spills at 64 registers than the unrolled stages
@@ -310,6 +327,19 @@ __global__ void __launch_bounds__(256, 4) fft_pass_inplace_kernel(const double2*
         }
     }
 }
+
+template <int SIGN, int R0, int R1, int R2, int R3, int P0, int P1, int P2, int P3>
+__global__ void __launch_bounds__(256, 4) fft_pass_inplace_kernel(const double2* src, double2* dst,
+                                                                  const FftPassArgs a)
+{
+    extern __shared__ double2 smem[];
+    if (a.srcs) {
+        src = a.srcs[blockIdx.z];
+        dst = a.dsts[blockIdx.z];
+    }
+    InplaceTile<SIGN, R0, R1, R2, R3, P0, P1, P2, P3>::run(a, blockIdx.x, blockIdx.y, src, dst, smem);
+}
+
 
 // Direct O(R^2) butterfly for any other radix (rare lengths with a large prime factor).
 template <int SIGN>
@@ -340,7 +370,7 @@ __device__ void run_stage_generic(const FftPassArgs& a, int s, const double2* gs
         for (int q = 0; q < R; ++q) {
             double2 acc = make_double2(0.0, 0.0);
             for (int r = 0; r < R; ++r) {
-                double2 x = first ? __ldg(gsrc + src_base + (long long)kk * a.src.sv + (long long)(j + r * m) * a.src.se)
+                double2 x = first ? load_src(a, gsrc + src_base + (long long)kk * a.src.sv + (long long)(j + r * m) * a.src.se)
                                   : sin_[kk * pl + spos(j + r * m)];
                 if (Ns > 1 && r > 0) x = cmul(x, twiddle(a.twiddle, r * k * step, SIGN));
                 const int e = (r * q) % R;
@@ -354,18 +384,20 @@ __device__ void run_stage_generic(const FftPassArgs& a, int s, const double2* gs
 }
 
 template <int SIGN>
-__global__ void __launch_bounds__(256, 2) fft_pass_kernel(const double2* src, double2* dst,
-                                                       const FftPassArgs a)
+struct PingPongTile {
+    static constexpr int kMinBlocks = 2;   // as the stand-alone kernel
+    static __device__ __forceinline__ void run(const FftPassArgs& a, int bx, int by, const double2* src, double2* dst,
+                                               double2* smem);
+};
+
+template <int SIGN>
+__device__ __forceinline__ void PingPongTile<SIGN>::run(const FftPassArgs& a, int bx, int by, const double2* src,
+                                                        double2* dst, double2* smem)
 {
-    extern __shared__ double2 smem[];
-    if (a.srcs) {
-        src = a.srcs[blockIdx.z];
-        dst = a.dsts[blockIdx.z];
-    }
-    const int v0 = blockIdx.x * a.kb;
+    const int v0 = bx * a.kb;
     const int nv = min(a.kb, a.nvec - v0);
-    const long long src_base = (long long)v0 * a.src.sv + (long long)blockIdx.y * a.src.sb;
-    const long long dst_base = (long long)v0 * a.dst.sv + (long long)blockIdx.y * a.dst.sb;
+    const long long src_base = (long long)v0 * a.src.sv + (long long)by * a.src.sb;
+    const long long dst_base = (long long)v0 * a.dst.sv + (long long)by * a.dst.sb;
     const int pl = padded_len(a.n);
     double2* buf[2] = {smem, smem + a.kb * pl};
     // In-place passes (src == dst) are safe: every CTA reads its whole tile in stage 0 and
@@ -385,6 +417,124 @@ __global__ void __launch_bounds__(256, 2) fft_pass_kernel(const double2* src, do
             default: run_stage_generic<SIGN>(a, s, src, dst, sin_, sout, nv, src_base, dst_base); break;
         }
         if (s + 1 < a.nstages) __syncthreads();
+    }
+}
+
+template <int SIGN>
+__global__ void __launch_bounds__(256, 2) fft_pass_kernel(const double2* src, double2* dst,
+                                                       const FftPassArgs a)
+{
+    extern __shared__ double2 smem[];
+    if (a.srcs) {
+        src = a.srcs[blockIdx.z];
+        dst = a.dsts[blockIdx.z];
+    }
+    PingPongTile<SIGN>::run(a, blockIdx.x, blockIdx.y, src, dst, smem);
+}
+
+// Both passes of one direction in one persistent launch. The layers (the vector index of both
+// passes) are cut into chunks; CTAs take work items in order from a counter: the first pass's
+// tiles of chunk 0, then for each chunk c >= 1 the first pass's tiles of chunk c followed by the
+// second pass's tiles of chunk c - 1, then the second pass of the last chunk; transforms of a
+// batch one after another. A second-pass tile of chunk c starts once all first-pass tiles of that
+// chunk have finished (a counter per chunk), so it reads the first pass's output of the chunk
+// while it is still in L2 and the workspace makes one HBM round trip instead of two. Every item
+// that waits comes after the items it waits for, and every CTA is resident, so the waits end; a
+// wait is bounded all the same (2 s), after which the tile runs anyway and the status word is set.
+struct FusedArgs {
+    FftPassArgs p[2];
+    const double2* src[2];   // single transform: each pass's source and destination
+    double2* dst[2];
+    int cx[2];               // vector tiles of each pass per chunk (chunk / kb)
+    int ny[2];               // tiles along the other index of each pass
+    int nchunks;             // chunks per transform
+    int per_z;               // items per transform
+    int total;               // items of the launch
+    long long sync_off;      // double2 offset of the counters in each transform's workspace
+    double2* ws;             // single transform: its workspace
+};
+
+// Counters of transform z: [0] next item and [1] status (transform 0 only), [2 + c] first-pass
+// tiles of chunk c that have finished. The workspace is the second pass's source.
+__device__ __forceinline__ int* fused_sync(const FusedArgs& f, int z)
+{
+    const double2* w = f.p[1].srcs ? f.p[1].srcs[z] : f.ws;
+    return reinterpret_cast<int*>(const_cast<double2*>(w) + f.sync_off);
+}
+
+__global__ void fused_sync_clear(FusedArgs f, int words)
+{
+    int* w = fused_sync(f, blockIdx.x);
+    for (int i = threadIdx.x; i < words; i += blockDim.x) w[i] = 0;
+}
+
+template <int SIGN, class Tile>
+__global__ void __launch_bounds__(256, Tile::kMinBlocks) fft_fused_kernel(const __grid_constant__ FusedArgs f)
+{
+    extern __shared__ double2 smem[];
+    __shared__ int s_item;
+    int* ctl = fused_sync(f, 0);
+    const int T1 = f.cx[0] * f.ny[0], T2 = f.cx[1] * f.ny[1];
+    for (;;) {
+        if (threadIdx.x == 0) s_item = atomicAdd(ctl, 1);
+        __syncthreads();
+        const int item = s_item;
+        __syncthreads();
+        if (item >= f.total) break;
+        const int z = item / f.per_z;
+        int j = item - z * f.per_z;
+        int pass, c, t;
+        if (j < T1) {
+            pass = 0;
+            c = 0;
+            t = j;
+        } else {
+            j -= T1;
+            const int step = 1 + j / (T1 + T2);
+            const int r = j - (step - 1) * (T1 + T2);
+            if (step < f.nchunks && r < T1) {
+                pass = 0;
+                c = step;
+                t = r;
+            } else {
+                pass = 1;
+                c = step - 1;
+                t = step < f.nchunks ? r - T1 : r;
+            }
+        }
+        int* done = fused_sync(f, z) + 2;
+        if (pass == 1) {
+            if (threadIdx.x == 0) {
+                const volatile int* d = done + c;
+                if (*d < T1) {
+                    uint64_t t0;
+                    asm volatile("mov.u64 %0, %globaltimer;" : "=l"(t0));
+                    for (;;) {
+                        if (*d >= T1) break;
+                        uint64_t t1;
+                        asm volatile("mov.u64 %0, %globaltimer;" : "=l"(t1));
+                        if (t1 - t0 > 2000000000ull) {
+                            atomicExch(ctl + 1, 1);
+                            break;
+                        }
+                        __nanosleep(256);
+                    }
+                }
+                __threadfence();
+            }
+            __syncthreads();
+        }
+        // one call site; the arguments are a __grid_constant__ parameter, so indexing them by the
+        // pass reads the parameter space instead of copying it to local memory
+        const FftPassArgs& a = f.p[pass];
+        const double2* src = a.srcs ? a.srcs[z] : f.src[pass];
+        double2* dst = a.dsts ? a.dsts[z] : f.dst[pass];
+        Tile::run(a, c * f.cx[pass] + t % f.cx[pass], t / f.cx[pass], src, dst, smem);
+        if (pass == 0) {
+            __threadfence();   // this thread's stores, before the count says the tile is done
+            __syncthreads();
+            if (threadIdx.x == 0) atomicAdd(done + c, 1);
+        }
     }
 }
 
@@ -524,6 +674,91 @@ cudaError_t fft_pass_launch(const double2* src, double2* dst, const FftPassArgs&
         sign < 0 ? go(fft_pass_kernel<-1>) : go(fft_pass_kernel<1>);
     }
     return cudaGetLastError();
+}
+
+bool g_fft_fused = true;
+bool fft_fused_enabled() { return g_fft_fused; }
+void fft_set_fused(bool on) { g_fft_fused = on; }
+
+// Layers per chunk of the fused passes: about 16 MB of workspace per chunk, a multiple of both
+// passes' tile vectors that divides the layer count; 0 when the passes cannot be fused.
+int fft_fused_chunk(const FftPassArgs& p0, const FftPassArgs& p1)
+{
+    if (p0.n != p1.n || p0.nvec != p1.nvec || p0.kb != p1.kb || p0.nstages != p1.nstages || p0.nstages == 0) return 0;
+    for (int st = 0; st < p0.nstages; ++st)
+        if (p0.radix[st] != p1.radix[st]) return 0;
+    const int nvec = p0.nvec, kb = p0.kb;
+    const long long layer_bytes = (long long)p0.n * p0.n * (long long)sizeof(double2);
+    int want = (int)((16ll << 20) / (layer_bytes > 0 ? layer_bytes : 1));
+    if (want < kb) want = kb;
+    int best = 0;
+    for (int c = kb; c <= nvec; c += kb)
+        if (nvec % c == 0 && c <= want) best = c;
+    if (best == 0 && nvec % kb == 0) best = kb;
+    if (best == 0 || 2 + nvec / best > kFftSyncBytes / (int)sizeof(int)) return 0;
+    return best;
+}
+
+cudaError_t fft_fused_launch(int sign, const FftPassArgs& p0, const FftPassArgs& p1, int ntiles0, int ntiles1, int nz,
+                             const double2* src0, double2* dst0, const double2* src1, double2* dst1, double2* ws,
+                             long long sync_off, cudaStream_t stream)
+{
+    const int chunk = fft_fused_chunk(p0, p1);
+    if (chunk == 0) return cudaErrorInvalidValue;
+    if (nz > 1 && !(p0.srcs && p0.dsts && p1.srcs && p1.dsts)) return cudaErrorInvalidValue;
+    FusedArgs f;
+    memset(&f, 0, sizeof(f));
+    f.p[0] = p0;
+    f.p[1] = p1;
+    f.p[1].coherent = 1;   // reads what the first pass's CTAs of this launch wrote
+    f.src[0] = src0;
+    f.dst[0] = dst0;
+    f.src[1] = src1;
+    f.dst[1] = dst1;
+    f.cx[0] = f.cx[1] = chunk / p0.kb;
+    f.ny[0] = ntiles0;
+    f.ny[1] = ntiles1;
+    f.nchunks = p0.nvec / chunk;
+    f.per_z = f.nchunks * (f.cx[0] * f.ny[0] + f.cx[1] * f.ny[1]);
+    f.total = f.per_z * nz;
+    f.sync_off = sync_off;
+    f.ws = ws;
+    fused_sync_clear<<<nz, 128, 0, stream>>>(f, 2 + f.nchunks);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    const InplacePlan* ip = inplace_plan_of(p0);
+    int widest = 1;
+    for (int st = 0; st < p0.nstages; ++st) widest = p0.n / p0.radix[st] > widest ? p0.n / p0.radix[st] : widest;
+    int nthreads = ((p0.kb * widest + 31) / 32) * 32;
+    if (ip || nthreads > 256) nthreads = 256;
+    const size_t smem = fft_pass_smem_bytes(p0);
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    auto go = [&](auto kern) -> cudaError_t {
+        if (smem > 48 * 1024) cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        int per = 1;
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kern, nthreads, smem) != cudaSuccess || per < 1) per = 1;
+        const int blocks = std::min(sms * per, f.total);
+        kern<<<blocks, nthreads, smem, stream>>>(f);
+        return cudaGetLastError();
+    };
+    if (ip) {
+        switch (ip->n) {
+            case 512: return sign < 0 ? go(fft_fused_kernel<-1, InplaceTile<-1, 8, 8, 8, 0, 1, 1, 1, 1>>)
+                                      : go(fft_fused_kernel<1, InplaceTile<1, 8, 8, 8, 0, 1, 1, 1, 1>>);
+            case 384: return sign < 0 ? go(fft_fused_kernel<-1, InplaceTile<-1, 8, 4, 4, 3, 1, 2, 2, 2>>)
+                                      : go(fft_fused_kernel<1, InplaceTile<1, 8, 4, 4, 3, 1, 2, 2, 2>>);
+            case 192: return sign < 0 ? go(fft_fused_kernel<-1, InplaceTile<-1, 8, 8, 3, 0, 1, 1, 2, 1>>)
+                                      : go(fft_fused_kernel<1, InplaceTile<1, 8, 8, 3, 0, 1, 1, 2, 1>>);
+            case 32: return sign < 0 ? go(fft_fused_kernel<-1, InplaceTile<-1, 8, 4, 0, 0, 1, 1, 1, 1>>)
+                                     : go(fft_fused_kernel<1, InplaceTile<1, 8, 4, 0, 0, 1, 1, 1, 1>>);
+            case 96: return sign < 0 ? go(fft_fused_kernel<-1, InplaceTile<-1, 8, 4, 3, 0, 1, 1, 1, 1>>)
+                                     : go(fft_fused_kernel<1, InplaceTile<1, 8, 4, 3, 0, 1, 1, 1, 1>>);
+            default: return cudaErrorInvalidValue;
+        }
+    }
+    return sign < 0 ? go(fft_fused_kernel<-1, PingPongTile<-1>>) : go(fft_fused_kernel<1, PingPongTile<1>>);
 }
 
 }  // namespace pfsoft_dev

@@ -28,6 +28,7 @@ struct FftPassArgs {
     // batched passes: when set, transform z = blockIdx.z reads srcs[z] and writes dsts[z]
     const double2* const* srcs;
     double2* const* dsts;
+    int coherent;                // first-stage loads through the coherent path (0: read-only path)
 };
 
 // Radix plan for length n; returns the number of stages (0 if n cannot be planned).
@@ -39,6 +40,22 @@ cudaError_t fft_pass_launch(const double2* src, double2* dst, const FftPassArgs&
                             cudaStream_t stream, int nz = 1);
 
 size_t fft_pass_smem_bytes(const FftPassArgs& a);
+
+// Both passes of one direction in one persistent launch, chunk by chunk over the layers, so that
+// the second pass reads the first pass's output of a chunk from L2 (see fft.cu). p0 / p1: the
+// passes as fft_pass_launch takes them (same length, plan and tile vectors; ntiles0 / ntiles1
+// their tile counts), nz transforms (nz > 1: the pointer tables of both passes; nz == 1: the
+// pointers src0..dst1). Each transform's workspace -- the second pass's source, `ws` when nz == 1 --
+// holds kFftSyncBytes bytes of counters at double2 offset sync_off. Returns cudaErrorInvalidValue
+// when the passes cannot be fused (fft_fused_chunk == 0).
+constexpr int kFftSyncBytes = 4096;
+int fft_fused_chunk(const FftPassArgs& p0, const FftPassArgs& p1);
+// Whether the transforms use the fused launch (default on; pfsoft_tune_fft_fused).
+bool fft_fused_enabled();
+void fft_set_fused(bool on);
+cudaError_t fft_fused_launch(int sign, const FftPassArgs& p0, const FftPassArgs& p1, int ntiles0, int ntiles1, int nz,
+                             const double2* src0, double2* dst0, const double2* src1, double2* dst1, double2* ws,
+                             long long sync_off, cudaStream_t stream);
 
 // Vectors per tile for length n: 8 (128 contiguous bytes on the transposed side) unless the
 // ping-pong buffers of 8 vectors would leave a single CTA per SM, then 4; plans of three or more

@@ -241,16 +241,21 @@ int launch_split_batch(pfsoft_server* s, Batch* b, const std::vector<Request>& i
         if (io[i].ready) e = cudaStreamWaitEvent(sl.stream, io[i].ready, 0);
     if (e == cudaSuccess) e = cudaMemcpyAsync(sl.d_stage, sl.h_stage, s->stage_bytes, cudaMemcpyHostToDevice, sl.stream);
     const int sign = dir == 0 ? -1 : +1;
-    auto fft = [&](size_t g, bool first) {
-        const FftPassArgs a = group_pass_args(dir, first, tabs[g], d_tab + gbase[g], d_tab + 2 * cap + gbase[g]);
-        return fft_pass_launch(nullptr, nullptr, a, tabs[g].N, sign, sl.stream, gT[g]);
+    auto fft = [&](size_t g) -> cudaError_t {
+        const FftPassArgs a = group_pass_args(dir, true, tabs[g], d_tab + gbase[g], d_tab + 2 * cap + gbase[g]);
+        const FftPassArgs c = group_pass_args(dir, false, tabs[g], d_tab + gbase[g], d_tab + 2 * cap + gbase[g]);
+        const int N = tabs[g].N;
+        if (fft_fused_enabled() && fft_fused_chunk(a, c))
+            return fft_fused_launch(sign, a, c, N, N, gT[g], nullptr, nullptr, nullptr, nullptr, nullptr,
+                                    (long long)N * N * N + (long long)dwt_split_aux_elems(gB[g]), sl.stream);
+        cudaError_t e2 = fft_pass_launch(nullptr, nullptr, a, N, sign, sl.stream, gT[g]);
+        return e2 == cudaSuccess ? fft_pass_launch(nullptr, nullptr, c, N, sign, sl.stream, gT[g]) : e2;
     };
     for (size_t g = 0; g < tabs.size() && e == cudaSuccess; ++g) {
         double2** ws = d_tab + 2 * cap + gbase[g];
         double2** cf = d_tab + cap + gbase[g];
         if (dir == 0) {
-            e = fft(g, true);
-            if (e == cudaSuccess) e = fft(g, false);
+            e = fft(g);
         } else {
             e = zero_nyquist_launch(ws, gB[g], gT[g], sl.stream);
         }
@@ -258,10 +263,7 @@ int launch_split_batch(pfsoft_server* s, Batch* b, const std::vector<Request>& i
     }
     if (e == cudaSuccess)
         e = dwt_split_launch(dir, d_groups, sl.d_stage + groups_bytes, (int)tabs.size(), n_items, sl.d_status, sl.stream);
-    for (size_t g = 0; dir == 1 && g < tabs.size() && e == cudaSuccess; ++g) {
-        e = fft(g, true);
-        if (e == cudaSuccess) e = fft(g, false);
-    }
+    for (size_t g = 0; dir == 1 && g < tabs.size() && e == cudaSuccess; ++g) e = fft(g);
     if (e == cudaSuccess) e = cudaLaunchHostFunc(sl.stream, on_batch_done, b);
     if (e != cudaSuccess) return fail(PFSOFT_ECUDA, std::string("server split batch: ") + cudaGetErrorString(e));
     return PFSOFT_OK;
@@ -538,6 +540,7 @@ int pfsoft_server_submit(pfsoft_server* s, int direction, int B, const double* d
     if (!d_in || !d_out) return fail(PFSOFT_EINVAL, "null buffer");
     if ((reinterpret_cast<uintptr_t>(d_in) & 15) || (reinterpret_cast<uintptr_t>(d_out) & 15))
         return fail(PFSOFT_EINVAL, "buffers must be 16-byte aligned");
+    // pfsoft_workspace_bytes includes the FFT counters; in split mode they follow the scale table
     const size_t bytes = pfsoft_workspace_bytes(B) + (s->split ? dwt_split_aux_elems(B) * sizeof(double2) : 0);
     {
         std::lock_guard<std::mutex> lk(s->mu);

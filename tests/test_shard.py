@@ -350,6 +350,19 @@ def test_emulated_ranks_match_single_gpu(lib, B, P, mode):
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("B,P,mode", [(8, 3, "scatter"), (13, 4, "pack")])
+def test_emulated_ranks_match_oracle(lib, oracle, B, P, mode):
+    """The sharded forward and inverse against the long-double oracle's DSOFT / IDSOFT."""
+    from oracle import oracle as orc
+
+    g, coef, back = _emulate(B, P, mode)
+    g_h = g.cpu().numpy()
+    f_ref = oracle.dsoft(g_h)
+    assert orc.rel_l2(coef.cpu().numpy(), f_ref) <= 1e-13
+    assert orc.rel_l2(back.cpu().numpy(), oracle.idsoft(coef.cpu().numpy(), B)) <= 1e-13
+
+
+@pytest.mark.gpu
 def test_sharded_transform_one_rank_nccl(lib):
     """ShardedTransform end to end through NCCL (a one-rank group: the collectives run, the
     exchange is a self-copy) against the unsharded transform."""
