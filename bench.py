@@ -328,6 +328,15 @@ def mixed_section(lib, steps: int, warmup: int, tune: bool = False) -> dict:
     split_grid_vs = max(_rel(grids[i], g64[i]) for i in range(len(bws)))
     split_coef_vs = max(_rel(back[i], c64[i]) for i in range(len(bws)))
     split_rt = max(_rel(back[i], coeffs[i]) for i in range(len(bws)))
+    # the autotuned plan: per bandwidth, the FFT stage fused or not and the DWT split or FP64
+    tuned = autotune.tune_plan(lib, bws, coeffs, grids, back, use_cache=False)
+    ptu = _Plan(lib, bws, SPLIT)
+    ms_tuned = _timed(lambda: (ptu.idsoft(coeffs, grids, s), ptu.dsoft(grids, back, s)), steps, warmup)
+    ptu.close()
+    torch.cuda.synchronize()
+    tuned_vs = max(_rel(back[i], c64[i]) for i in range(len(bws)))
+    lib.pfsoft_tune_fft_fused(0, 1)        # back to the defaults for what follows
+    lib.pfsoft_tune_split_bandwidth(0, 1)
     # the oracle on the first B = 32 transform (long double, all on the host)
     i32 = bws.index(32)
     ora = orc.Oracle()
@@ -363,6 +372,8 @@ def mixed_section(lib, steps: int, warmup: int, tune: bool = False) -> dict:
                        "rel_l2_vs_plain_max": batch_vs, "transforms_per_cta": tpc or "default", "autotune_ms": tune_ms},
         "split_batch": {"value": tps(ms_split), "ms_per_step": ms_split, "speedup_vs_plain_loop": ms_plain / ms_split,
                         "status": split_status},
+        "tuned_batch": {"value": tps(ms_tuned), "ms_per_step": ms_tuned, "speedup_vs_plain_loop": ms_plain / ms_tuned,
+                        "rel_l2_vs_fp64_max": tuned_vs, "autotune": tuned},
         "split_served": {"value": sat["transforms_per_s"], "speedup_vs_plain_loop": sat["transforms_per_s"] / tps(ms_plain),
                          "p50_ms": sat["p50_ms"], "p99_ms": sat["p99_ms"], "mean_batch": sat["mean_batch"],
                          "max_concurrent_batches": sat["max_concurrent_batches"],

@@ -278,8 +278,13 @@ long long pfsoft_launch_count(void);
 int pfsoft_tune_dwt_case_split(int direction, int case_split);
 /* Tuning knob: on != 0 (the default) runs the two FFT passes of a direction in one persistent
  * launch, layer chunk by layer chunk, so that the second pass reads the first pass's output from
- * L2; 0 runs them as two launches. Process-wide; for measurements and the autotuner. */
-int pfsoft_tune_fft_fused(int on);
+ * L2; 0 runs them as two launches. For bandwidth B (B <= 0: every bandwidth, clearing the
+ * per-bandwidth choices). Process-wide; for measurements and the autotuner. */
+int pfsoft_tune_fft_fused(int B, int on);
+/* Tuning knob: whether a plan created with PFSOFT_BATCH_SPLIT runs bandwidth B's DWT on the split
+ * kernel (use_split != 0, the default) or on the FP64 kernels (0). B <= 0: every bandwidth,
+ * clearing the per-bandwidth choices. Set by the autotuner; read when a plan is created. */
+int pfsoft_tune_split_bandwidth(int B, int use_split);
 /* Test knob for the split-precision DWT's failure path (no counterpart in the reference): when
  * wait_ns > 0, every later split launch first waits up to wait_ns nanoseconds on a barrier that
  * nothing signals, before it issues any MMA; the wait runs out, every warp of the kernel leaves,

@@ -46,7 +46,8 @@ SIGNATURES = {
     "pfsoft_cuda_random_coeffs": (_c_int, [_vp, _c_int, ctypes.c_ulonglong, _c_int, _c_double, _vp]),
     "pfsoft_launch_count": (ctypes.c_longlong, []),
     "pfsoft_tune_dwt_case_split": (_c_int, [_c_int, _c_int]),
-    "pfsoft_tune_fft_fused": (_c_int, [_c_int]),
+    "pfsoft_tune_fft_fused": (_c_int, [_c_int, _c_int]),
+    "pfsoft_tune_split_bandwidth": (_c_int, [_c_int, _c_int]),
     "pfsoft_test_split_wait_ns": (_c_int, [ctypes.c_ulonglong]),
     "pfsoft_server_create": (_c_int, [_c_size, _c_int, _c_int, _vp]),
     "pfsoft_server_create_ex": (_c_int, [_c_size, _c_int, _c_int, _c_int, _vp]),

@@ -270,7 +270,7 @@ int run_dsoft(const double* d_grid, int B, double* d_coeffs, void* ws, cudaStrea
     // F2: vectors = layers k, tile = gamma bin r, elements = column c; in place on X
     FftPassArgs f2 = pass_args(N, N, t, FftStrides{1, n2, n}, FftStrides{1, n2, n}, 1.0);
     if (f1.nstages == 0) return fail(PFSOFT_EINVAL, "FFT length cannot be planned");
-    if (fft_fused_enabled() && fft_fused_chunk(f1, f2)) {
+    if (fft_fused_enabled(N) && fft_fused_chunk(f1, f2)) {
         // both passes in one launch; the counters sit past the spectrum in the workspace
         StageScope sc(ST_FFT_FWD_FUSED, s);
         PF_CUDA(fft_fused_launch(-1, f1, f2, N, N, 1, G, X, X, X, X, (long long)grid_elems(B), s));
@@ -315,7 +315,7 @@ int run_idsoft(const double* d_coeffs, int B, double* d_grid, void* ws, cudaStre
     // I1: inverse DFT over gamma, X[r][c][k] -> G[k][c][r], scaled by 1/(4B^2) (src/fn_idsoft.cpp:289)
     FftPassArgs i1 = pass_args(N, N, t, FftStrides{1, n, n2}, FftStrides{n2, n, 1}, 1.0 / (4.0 * B * B));
     if (i1.nstages == 0) return fail(PFSOFT_EINVAL, "FFT length cannot be planned");
-    if (fft_fused_enabled() && fft_fused_chunk(i2, i1)) {
+    if (fft_fused_enabled(N) && fft_fused_chunk(i2, i1)) {
         StageScope sc(ST_FFT_INV_FUSED, s);
         PF_CUDA(fft_fused_launch(+1, i2, i1, N, N, 1, X, X, X, G, X, (long long)grid_elems(B), s));
     } else {
@@ -661,9 +661,10 @@ int pfsoft_cuda_wigner_d_matrix(int B, int M, int Mp, int weighted, double* d_ou
 
 long long pfsoft_launch_count(void) { return g_launches.load(); }
 
-int pfsoft_tune_fft_fused(int on)
+int pfsoft_tune_fft_fused(int B, int on)
 {
-    fft_set_fused(on != 0);
+    if (B > kMaxBandwidth) return fail(PFSOFT_EINVAL, "bandwidth must be at most 512");
+    fft_set_fused(B <= 0 ? 0 : 2 * B, on);
     return PFSOFT_OK;
 }
 

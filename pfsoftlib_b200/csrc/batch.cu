@@ -35,6 +35,17 @@ namespace {
 
 constexpr int kBatchMaxFused = 128;   // largest bandwidth of the fused DWT launch (N <= 256)
 
+// Autotuner's split-precision choice per bandwidth (0 default = split where supported, 1 split,
+// -1 FP64), read when a PFSOFT_BATCH_SPLIT plan is created.
+signed char g_split_choice[513] = {};
+bool g_split_all = true;
+
+bool split_wanted(int B)
+{
+    if (B >= 1 && B <= 512 && g_split_choice[B]) return g_split_choice[B] > 0;
+    return g_split_all;
+}
+
 __global__ void zero_nyquist_batched(double2* const* X, int B)
 {
     double2* x = X[blockIdx.z];
@@ -137,7 +148,7 @@ int launch_group(int dir, const BandTables& t, int T, double2** d_grids, double2
     // both passes of the direction: one fused launch (counters past each spectrum) or two
     auto passes = [&]() -> cudaError_t {
         const FftPassArgs a = group_pass_args(dir, true, t, d_grids, d_ws), b = group_pass_args(dir, false, t, d_grids, d_ws);
-        if (fft_fused_enabled() && fft_fused_chunk(a, b))
+        if (fft_fused_enabled(t.N) && fft_fused_chunk(a, b))
             return fft_fused_launch(sign, a, b, t.N, t.N, T, nullptr, nullptr, nullptr, nullptr, nullptr,
                                     (long long)t.N * t.N * t.N, s);
         cudaError_t e = pass(true);
@@ -240,7 +251,7 @@ int enqueue(pfsoft_batch* b, int dir, cudaStream_t s)
     auto fft_both = [&](const pfsoft_batch::Group& g) -> cudaError_t {
         const FftPassArgs a = group_pass_args(dir, true, g.tables, b->grid_ptrs() + g.ptr_base, b->ws_ptrs() + g.ptr_base);
         const FftPassArgs c = group_pass_args(dir, false, g.tables, b->grid_ptrs() + g.ptr_base, b->ws_ptrs() + g.ptr_base);
-        if (fft_fused_enabled() && fft_fused_chunk(a, c))
+        if (fft_fused_enabled(g.N) && fft_fused_chunk(a, c))
             return fft_fused_launch(sign, a, c, g.N, g.N, (int)g.members.size(), nullptr, nullptr, nullptr, nullptr, nullptr,
                                     (long long)g.N * g.N * g.N + (g.split ? (long long)dwt_split_aux_elems(g.B) : 0), s);
         cudaError_t e = fft_group(g, true);
@@ -339,7 +350,7 @@ int pfsoft_batch_create(const int* bandwidths, int count, int transforms_per_cta
         g.members = kv.second;
         g.ptr_base = base;
         base += g.members.size();
-        g.split = (flags & PFSOFT_BATCH_SPLIT) && dwt_split_supported(g.B);
+        g.split = (flags & PFSOFT_BATCH_SPLIT) && dwt_split_supported(g.B) && split_wanted(g.B);
         for (int t : g.members) {
             ws_off[t] = ws_total;
             ws_total += ((size_t)g.N * g.N * g.N + (g.split ? dwt_split_aux_elems(g.B) : 0)) * sizeof(double2) + kFftSyncBytes;
@@ -475,6 +486,18 @@ size_t pfsoft_batch_workspace_bytes(const pfsoft_batch* b) { return b ? b->ws_by
 int pfsoft_batch_transforms_per_cta(const pfsoft_batch* b) { return b ? b->tpc : 0; }
 
 int pfsoft_split_supported(int B) { return dwt_split_supported(B) ? 1 : 0; }
+
+int pfsoft_tune_split_bandwidth(int B, int use_split)
+{
+    if (B > 512) return fail(PFSOFT_EINVAL, "bandwidth must be at most 512");
+    if (B <= 0) {
+        g_split_all = use_split != 0;
+        for (auto& v : g_split_choice) v = 0;
+    } else {
+        g_split_choice[B] = use_split ? 1 : -1;
+    }
+    return PFSOFT_OK;
+}
 
 int pfsoft_test_split_wait_ns(unsigned long long wait_ns)
 {

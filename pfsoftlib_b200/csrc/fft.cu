@@ -676,9 +676,24 @@ cudaError_t fft_pass_launch(const double2* src, double2* dst, const FftPassArgs&
     return cudaGetLastError();
 }
 
-bool g_fft_fused = true;
-bool fft_fused_enabled() { return g_fft_fused; }
-void fft_set_fused(bool on) { g_fft_fused = on; }
+// Fused-pass choice per transform length (index n <= 1024; default on), set by the autotuner.
+constexpr int kFusedMaxN = 1024;
+signed char g_fft_fused[kFusedMaxN + 1] = {};   // 0 default (on), 1 on, -1 off
+bool g_fft_fused_all = true;
+bool fft_fused_enabled(int n)
+{
+    if (n >= 0 && n <= kFusedMaxN && g_fft_fused[n]) return g_fft_fused[n] > 0;
+    return g_fft_fused_all;
+}
+void fft_set_fused(int n, int on)
+{
+    if (n <= 0) {
+        g_fft_fused_all = on != 0;
+        for (int i = 0; i <= kFusedMaxN; ++i) g_fft_fused[i] = 0;
+    } else if (n <= kFusedMaxN) {
+        g_fft_fused[n] = on ? 1 : -1;
+    }
+}
 
 // Layers per chunk of the fused passes: about 16 MB of workspace per chunk, a multiple of both
 // passes' tile vectors that divides the layer count; 0 when the passes cannot be fused.

@@ -50,9 +50,10 @@ size_t fft_pass_smem_bytes(const FftPassArgs& a);
 // when the passes cannot be fused (fft_fused_chunk == 0).
 constexpr int kFftSyncBytes = 4096;
 int fft_fused_chunk(const FftPassArgs& p0, const FftPassArgs& p1);
-// Whether the transforms use the fused launch (default on; pfsoft_tune_fft_fused).
-bool fft_fused_enabled();
-void fft_set_fused(bool on);
+// Whether transforms of length n use the fused launch (default on; pfsoft_tune_fft_fused sets it
+// per length, or for every length with n <= 0).
+bool fft_fused_enabled(int n);
+void fft_set_fused(int n, int on);
 cudaError_t fft_fused_launch(int sign, const FftPassArgs& p0, const FftPassArgs& p1, int ntiles0, int ntiles1, int nz,
                              const double2* src0, double2* dst0, const double2* src1, double2* dst1, double2* ws,
                              long long sync_off, cudaStream_t stream);

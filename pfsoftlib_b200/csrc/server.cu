@@ -245,7 +245,7 @@ int launch_split_batch(pfsoft_server* s, Batch* b, const std::vector<Request>& i
         const FftPassArgs a = group_pass_args(dir, true, tabs[g], d_tab + gbase[g], d_tab + 2 * cap + gbase[g]);
         const FftPassArgs c = group_pass_args(dir, false, tabs[g], d_tab + gbase[g], d_tab + 2 * cap + gbase[g]);
         const int N = tabs[g].N;
-        if (fft_fused_enabled() && fft_fused_chunk(a, c))
+        if (fft_fused_enabled(N) && fft_fused_chunk(a, c))
             return fft_fused_launch(sign, a, c, N, N, gT[g], nullptr, nullptr, nullptr, nullptr, nullptr,
                                     (long long)N * N * N + (long long)dwt_split_aux_elems(gB[g]), sl.stream);
         cudaError_t e2 = fft_pass_launch(nullptr, nullptr, a, N, sign, sl.stream, gT[g]);

@@ -16,3 +16,22 @@ def test_cache_roundtrip(tmp_path):
     autotune.store("k", 4, p)
     autotune.store("j", 2, p)
     assert autotune.load_cache(p) == {"k": 4, "j": 2}
+
+
+class _FakeLib:
+    def __init__(self):
+        self.calls = []
+
+    def pfsoft_tune_fft_fused(self, b, on):
+        self.calls.append(("fft", b, on))
+        return 0
+
+    def pfsoft_tune_split_bandwidth(self, b, on):
+        self.calls.append(("split", b, on))
+        return 0
+
+
+def test_apply_sets_per_bandwidth_knobs():
+    lib = _FakeLib()
+    autotune.apply(lib, {"fft_fused": {"64": True, "96": False}, "split": {"128": True}})
+    assert ("fft", 64, 1) in lib.calls and ("fft", 96, 0) in lib.calls and ("split", 128, 1) in lib.calls

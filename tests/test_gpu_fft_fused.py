@@ -32,12 +32,12 @@ def _round_trip(lib, B, c):
 def test_fused_equals_two_passes(lib, B):
     c = _coeffs(lib, B, 500 + B)
     try:
-        assert lib.pfsoft_tune_fft_fused(0) == 0
+        assert lib.pfsoft_tune_fft_fused(0, 0) == 0
         g2, f2 = _round_trip(lib, B, c)
-        assert lib.pfsoft_tune_fft_fused(1) == 0
+        assert lib.pfsoft_tune_fft_fused(0, 1) == 0
         g1, f1 = _round_trip(lib, B, c)
     finally:
-        lib.pfsoft_tune_fft_fused(1)
+        lib.pfsoft_tune_fft_fused(0, 1)
     assert torch.equal(g1, g2), f"B={B}: iDSOFT grids differ"
     assert torch.equal(f1, f2), f"B={B}: DSOFT coefficients differ"
     assert (torch.linalg.vector_norm(f1 - c) / torch.linalg.vector_norm(c)).item() <= 1e-13
@@ -51,7 +51,7 @@ def test_fused_batch_equals_two_passes(lib, split):
     out = {}
     try:
         for fused in (0, 1):
-            assert lib.pfsoft_tune_fft_fused(fused) == 0
+            assert lib.pfsoft_tune_fft_fused(0, fused) == 0
             plan = ctypes.c_void_p()
             assert lib.pfsoft_batch_create((ctypes.c_int * len(bws))(*bws), len(bws), 0, split | 1,
                                            ctypes.byref(plan)) == 0, lib.pfsoft_last_error()
@@ -67,7 +67,7 @@ def test_fused_batch_equals_two_passes(lib, split):
             lib.pfsoft_batch_destroy(plan)
             out[fused] = (gs, fs)
     finally:
-        lib.pfsoft_tune_fft_fused(1)
+        lib.pfsoft_tune_fft_fused(0, 1)
     for i, B in enumerate(bws):
         assert torch.equal(out[0][0][i], out[1][0][i]), f"B={B}: grids differ"
         assert torch.equal(out[0][1][i], out[1][1][i]), f"B={B}: coefficients differ"
