@@ -436,6 +436,16 @@ int pfsoft_batch_create(const int* bandwidths, int count, int transforms_per_cta
         for (size_t i = 0; i < g.members.size(); ++i)
             b->h_ptr[2 * (size_t)count + g.ptr_base + i] =
                 reinterpret_cast<double2*>(static_cast<char*>(b->ws) + ws_off[g.members[i]]);
+    // the fused FFT counters start cleared (a group whose FFT runs as two passes never writes them)
+    for (const auto& g : b->groups) {
+        const size_t sync = ((size_t)g.N * g.N * g.N + (g.split ? dwt_split_aux_elems(g.B) : 0)) * sizeof(double2);
+        for (size_t i = 0; i < g.members.size() && e == cudaSuccess; ++i)
+            e = cudaMemset(static_cast<char*>(b->ws) + ws_off[g.members[i]] + sync, 0, kFftSyncBytes);
+    }
+    if (e != cudaSuccess) {
+        free_batch(b);
+        return fail(PFSOFT_ECUDA, std::string("batch setup: ") + cudaGetErrorString(e));
+    }
     // group descriptors for the fused DWT (pointer tables inside the device array)
     for (size_t gi = 0; gi < b->groups.size(); ++gi) {
         const auto& g = b->groups[gi];
@@ -512,7 +522,18 @@ int pfsoft_batch_status(pfsoft_batch* b)
     cudaError_t e = cudaDeviceSynchronize();
     if (e == cudaSuccess) e = cudaMemcpy(st, b->d_split, sizeof(st), cudaMemcpyDeviceToHost);
     if (e != cudaSuccess) return fail(PFSOFT_ECUDA, std::string("batch status: ") + cudaGetErrorString(e));
-    return st[1] ? fail(PFSOFT_ETIMEOUT, "a bounded wait in the split-precision DWT ran out") : PFSOFT_OK;
+    if (st[1]) return fail(PFSOFT_ETIMEOUT, "a bounded wait in the split-precision DWT ran out");
+    // the fused FFT launches' status word (counters past the first transform's spectrum of each
+    // group, cleared by every launch): a bounded wait of the last execution ran out
+    for (const auto& g : b->groups) {
+        const char* ws = reinterpret_cast<const char*>(b->h_ptr[2 * (size_t)b->count + g.ptr_base]);
+        const size_t off = ((size_t)g.N * g.N * g.N + (g.split ? dwt_split_aux_elems(g.B) : 0)) * sizeof(double2);
+        int word = 0;
+        e = cudaMemcpy(&word, ws + off + sizeof(int), sizeof(int), cudaMemcpyDeviceToHost);
+        if (e != cudaSuccess) return fail(PFSOFT_ECUDA, std::string("batch status: ") + cudaGetErrorString(e));
+        if (word) return fail(PFSOFT_ETIMEOUT, "a bounded wait in the fused FFT launch ran out");
+    }
+    return PFSOFT_OK;
 }
 
 static int batch_run(pfsoft_batch* b, int dir, const double* const* in, double* const* out, void* stream)
