@@ -335,7 +335,7 @@ def mixed_section(lib, steps: int, warmup: int, tune: bool = False) -> dict:
     ptu.close()
     torch.cuda.synchronize()
     tuned_vs = max(_rel(back[i], c64[i]) for i in range(len(bws)))
-    lib.pfsoft_tune_fft_fused(0, 1)        # back to the defaults for what follows
+    lib.pfsoft_tune_fft_fused(0, 0)        # back to the defaults for what follows
     lib.pfsoft_tune_split_bandwidth(0, 1)
     # the oracle on the first B = 32 transform (long double, all on the host)
     i32 = bws.index(32)

@@ -276,9 +276,9 @@ long long pfsoft_launch_count(void);
 /* Tuning knob used by the autotuner: direction 0 = DSOFT, 1 = IDSOFT; case_split 1 = each warp
  * applies all eight symmetry cases, 2 = warp pairs split them, 0 = library default. */
 int pfsoft_tune_dwt_case_split(int direction, int case_split);
-/* Tuning knob: on != 0 (the default) runs the two FFT passes of a direction in one persistent
- * launch, layer chunk by layer chunk, so that the second pass reads the first pass's output from
- * L2; 0 runs them as two launches. For bandwidth B (B <= 0: every bandwidth, clearing the
+/* Tuning knob: on != 0 runs the two FFT passes of a direction in one persistent launch, layer
+ * chunk by layer chunk, so that the second pass reads the first pass's output from L2; 0 (the
+ * default) runs them as two launches. For bandwidth B (B <= 0: every bandwidth, clearing the
  * per-bandwidth choices). Process-wide; for measurements and the autotuner. */
 int pfsoft_tune_fft_fused(int B, int on);
 /* Tuning knob: whether a plan created with PFSOFT_BATCH_SPLIT runs bandwidth B's DWT on the split

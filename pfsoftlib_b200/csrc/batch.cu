@@ -353,7 +353,8 @@ int pfsoft_batch_create(const int* bandwidths, int count, int transforms_per_cta
         g.split = (flags & PFSOFT_BATCH_SPLIT) && dwt_split_supported(g.B) && split_wanted(g.B);
         for (int t : g.members) {
             ws_off[t] = ws_total;
-            ws_total += ((size_t)g.N * g.N * g.N + (g.split ? dwt_split_aux_elems(g.B) : 0)) * sizeof(double2) + kFftSyncBytes;
+            ws_total += ((((size_t)g.N * g.N * g.N + (g.split ? dwt_split_aux_elems(g.B) : 0)) * sizeof(double2) + kFftSyncBytes
+                          + 255) & ~(size_t)255);   // each workspace 256-byte aligned
         }
         int rc = tables_for(g.B, nullptr, &g.tables);
         if (rc) {

@@ -82,7 +82,8 @@ constexpr int kABytes = kPlanes * kAPlane;          // 24 KB
 constexpr int kBRows = 16 * kNT * kPlanes;          // 192
 constexpr int kBBytes = kBRows / 8 * 256;           // 6 KB
 constexpr int kStageBytes = kABytes + kBBytes;
-constexpr int kOffBar = kStages * kStageBytes;
+constexpr int kOffCoef = kStages * kStageBytes;     // generators: 32 steps x {c1, f1 f2, f1, row scale} per warp
+constexpr int kOffBar = kOffCoef + kGenWarps * 32 * 4 * 8;
 // mbarriers: full[kStages], empty[kStages], accfull[2], accempty[2], drain, never (test knob)
 constexpr int kBarFull = 0, kBarEmpty = kStages, kBarAccFull = 2 * kStages, kBarAccEmpty = 2 * kStages + kAccSets,
               kBarDrain = 2 * kStages + 2 * kAccSets, kBarNever = kBarDrain + 1, kNumBars = kBarNever + 1;
@@ -344,8 +345,13 @@ __global__ void __launch_bounds__(kThreads, 1)
                 unsigned char* Bm = smem + s * kStageBytes + kABytes;
                 constexpr int kTasks = 8 * kNT * 4;   // column pairs x octets
                 double raw[kTasks / 32][8][2];
+                double2 mxv[kTasks / 32];   // the column's largest |re|, |im| (operand-scale table)
                 int tq[kTasks / 32], to[kTasks / 32];
-                // loads first (they fly while the stage is still being read by the MMAs)
+                // loads first (they fly while the stage is still being read by the MMAs): the data,
+                // the columns' scale-table entries, and (inverse) the row scale of degree
+                // M + 32c + lane, handed to the lanes that need it by shuffles below
+                double irs_lane = 0.0;
+                if (DIR == 1 && c * kKC + lane < it.R) irs_lane = __ldg(&row_table(it.gr, it.t0)[it.M + c * kKC + lane].y);
 #pragma unroll
                 for (int i = 0; i < kTasks / 32; ++i) {
                     const int e = lane + 32 * i;
@@ -354,6 +360,12 @@ __global__ void __launch_bounds__(kThreads, 1)
                     tq[i] = cpair;
                     to[i] = o;
                     const bool live = t < nt && q < it.nc;
+                    {
+                        const double2* aux = it.gr->X[it.t0 + (live ? t : 0)] + (size_t)N * N * N;
+                        const PairCase p = class_case(it.M, it.Mp, live ? q : 0, N);
+                        mxv[i] = live ? (DIR == 0 ? __ldg(aux + (size_t)p.row * N + p.col) : __ldg(aux + (size_t)it.cls * 8 + q))
+                                      : make_double2(0.0, 0.0);
+                    }
                     if (DIR == 0) {
                         const PairCase p = class_case(it.M, it.Mp, live ? q : 0, N);
                         const double2* col = it.gr->X[it.t0 + (live ? t : 0)] + ((size_t)p.row * N + p.col) * N;
@@ -383,17 +395,15 @@ __global__ void __launch_bounds__(kThreads, 1)
                 for (int i = 0; i < kTasks / 32; ++i) {
                     const int cpair = tq[i], o = to[i];
                     const int t = cpair >> 3, q = cpair & 7;
-                    if (t >= nt || q >= it.nc) continue;   // columns never stored: left as they are
-                    const double2* aux = it.gr->X[it.t0 + t] + (size_t)N * N * N;
-                    double2 mx;
-                    double sgn_norm = 1.0;
-                    PairCase p = class_case(it.M, it.Mp, q, N);
-                    if (DIR == 0) {
-                        mx = aux[(size_t)p.row * N + p.col];
-                    } else {
-                        mx = aux[(size_t)it.cls * 8 + q];
-                        sgn_norm = (double)(B * 2 * B) / kPi;   // src/fn_idsoft.cpp:109
+                    double irs8[8];
+                    if (DIR == 1) {
+#pragma unroll
+                        for (int j = 0; j < 8; ++j) irs8[j] = __shfl_sync(0xffffffffu, irs_lane, 8 * o + j);
                     }
+                    if (t >= nt || q >= it.nc) continue;   // columns never stored: left as they are
+                    const double2 mx = mxv[i];
+                    const double sgn_norm = DIR == 0 ? 1.0 : (double)(B * 2 * B) / kPi;   // src/fn_idsoft.cpp:109
+                    PairCase p = class_case(it.M, it.Mp, q, N);
                     double cs_re, cs_im, ics_unused;
                     column_scale(mx.x, cs_re, ics_unused);
                     column_scale(mx.y, cs_im, ics_unused);
@@ -406,12 +416,11 @@ __global__ void __launch_bounds__(kThreads, 1)
                         }
                     } else {
                         // G = norm * sign(l) * f / (row scale), zero past the last degree
-                        const double2* rows = row_table(it.gr, it.t0);
 #pragma unroll
                         for (int j = 0; j < 8; ++j) {
                             const int l = it.M + c * kKC + 8 * o + j;
                             double f = 0.0;
-                            if (l < B) f = sgn_norm * case_sign(p, l, it.M) * __ldg(&rows[l].y);
+                            if (l < B) f = sgn_norm * case_sign(p, l, it.M) * irs8[j];
                             zr[j] = fma(f * raw[i][j][0], cs_re, kMagic);
                             zi[j] = fma(f * raw[i][j][1], cs_im, kMagic);
                         }
@@ -454,6 +463,17 @@ __global__ void __launch_bounds__(kThreads, 1)
             double rowf = 0.0;
             if (DIR == 0 && live) rowf = (kPi / (double)(B * 2 * B)) * __ldg(&row_table(it.gr, it.t0)[l].y);   // src/fn_dsoft.cpp:119
             for (int t = 0; t < it.nt; ++t) {
+                // the eight columns' scale-table entries, in flight while the accumulators are read
+                const double2* aux = it.gr->X[it.t0 + t] + (size_t)N * N * N;
+                double2 mxq[8];
+#pragma unroll
+                for (int q = 0; q < 8; ++q) {
+                    mxq[q] = make_double2(0.0, 0.0);
+                    if (q < it.nc) {
+                        const PairCase p = class_case(it.M, it.Mp, q, N);
+                        mxq[q] = DIR == 0 ? __ldg(aux + (size_t)p.row * N + p.col) : __ldg(aux + (size_t)it.cls * 8 + q);
+                    }
+                }
                 int32_t acc[kPlanes][16];
 #pragma unroll
                 for (int e = 0; e < kPlanes; ++e) tc::tmem_ld16(taddr + (uint32_t)(cols * e + 16 * t), acc[e]);
@@ -469,12 +489,11 @@ __global__ void __launch_bounds__(kThreads, 1)
                     v[j] = fma(h, 0x1p-8, (double)acc[0][j]) * 0x1p-14;
                 }
                 if (!live) continue;
-                const double2* aux = it.gr->X[it.t0 + t] + (size_t)N * N * N;
 #pragma unroll
                 for (int q = 0; q < 8; ++q) {
                     if (q >= it.nc) break;
                     const PairCase p = class_case(it.M, it.Mp, q, N);
-                    const double2 mx = DIR == 0 ? aux[(size_t)p.row * N + p.col] : aux[(size_t)it.cls * 8 + q];
+                    const double2 mx = mxq[q];
                     double unused, ics_re, ics_im;
                     column_scale(mx.x, unused, ics_re);
                     column_scale(mx.y, unused, ics_im);
@@ -494,20 +513,43 @@ __global__ void __launch_bounds__(kThreads, 1)
         }
     } else if (warp >= kGenWarp0) {
         // ------------------------------------------------------------------ generators (Wigner rows)
+        // The recurrence coefficients and row scales of 32 steps at a time are loaded by the warp's
+        // lanes in one coalesced load (a batch ahead, into registers) and published to the warp's
+        // shared-memory slot; the steps read them from there, so no step waits on global memory.
         const int w = warp - kGenWarp0;
+        double* s_cf = reinterpret_cast<double*>(smem + kOffCoef) + w * 128;
+        double2 pcf = make_double2(0.0, 0.0);
+        double pf1 = 0.0, prs = 0.0;
+        auto fetch = [&](const DwtGroup* gr, long long rc0, const double2* rows, int M, int R, int base) {
+            const int rr = base + lane;
+            pcf = make_double2(0.0, 0.0);
+            pf1 = 0.0;
+            prs = 0.0;
+            if (rr < R) {
+                pcf = __ldg(gr->rc_cf + rc0 + rr);
+                pf1 = __ldg(gr->rc_f1 + rc0 + rr);
+                prs = __ldg(&rows[M + rr].x);
+            }
+        };
+        auto publish = [&]() {
+            __syncwarp();
+            *reinterpret_cast<double2*>(s_cf + 4 * lane) = pcf;
+            *reinterpret_cast<double2*>(s_cf + 4 * lane + 2) = make_double2(pf1, prs);
+            __syncwarp();
+        };
         int g = 0;
         for (int r = 0;; ++r) {
             const int idx = cta_item(r, n_items);
             if (idx < 0 || *s_abort) break;
             const ItemGeo it = item_geo<DIR>(groups, segs, nseg, idx);
-            const int N = it.N;
+            const int N = it.N, R = it.R, M = it.M;
             const DwtGroup* gr = it.gr;
             const long long rc0 = rc_offset(it.B, it.M, it.Mp);
             const double nf = gr->normf[it.cls];
             const double2* rows = row_table(gr, it.t0);
             if (DIR == 0) {
                 // forward: this warp's chunks (beta columns 32c + lane), rows of the item's tile
-                const int r0 = 128 * it.tile, rn = min(it.R - r0, 128);
+                const int r0 = 128 * it.tile, rn = min(R - r0, 128), end = r0 + rn;
                 for (int c = 0; c < it.nchunks; ++c, ++g) {
                     if ((g % kGenWarps) != w) continue;
                     const int s = g % kStages, u = g / kStages;
@@ -519,24 +561,36 @@ __global__ void __launch_bounds__(kThreads, 1)
                         dcur = seed_value(nf * gr->w[k], gr->pw_sin[(size_t)(it.M - it.Mp) * N + k],
                                           gr->pw_cos[(size_t)(it.M + it.Mp) * N + k], sc);
                     }
-                    for (int rr = 0; rr < r0; ++rr)   // second row tile: run through the first 128 degrees
-                        rec_step(dcur, dprev, sc, cb, __ldg(gr->rc_cf + rc0 + rr), __ldg(gr->rc_f1 + rc0 + rr));
+                    fetch(gr, rc0, rows, M, R, 0);
+                    int base = 0;
+                    for (; base < r0; base += 32) {   // second row tile: run through the first 128 degrees
+                        publish();
+                        fetch(gr, rc0, rows, M, R, base + 32);
+#pragma unroll 8
+                        for (int j = 0; j < 32; ++j)
+                            rec_step(dcur, dprev, sc, cb, *reinterpret_cast<const double2*>(s_cf + 4 * j), s_cf[4 * j + 2]);
+                    }
                     if (!tc::mbar_wait_bounded(&bars[kBarEmpty + s], (uint32_t)((u & 1) ^ 1), kWaitNs, s_abort)) break;
                     unsigned char* A = smem + s * kStageBytes + lane * 16;   // (k/8)*128 + (k%8)*16 = lane*16
-                    if (k < N) {
-                        for (int r16 = 0; r16 < rn; r16 += 16) {
+                    for (; base < end; base += 32) {
+                        publish();
+                        fetch(gr, rc0, rows, M, R, base + 32);
+#pragma unroll 1
+                        for (int h = 0; h < 2; ++h) {
+                            const int b16 = base + 16 * h;
+                            if (b16 >= end) break;
                             double z[16];
 #pragma unroll
                             for (int j = 0; j < 16; ++j) {
-                                const int rr = r0 + r16 + j;
-                                if (rr < it.R) {
-                                    z[j] = fma(sc ? 0.0 : dcur, __ldg(&rows[it.M + rr].x), kMagic);
-                                    rec_step(dcur, dprev, sc, cb, __ldg(gr->rc_cf + rc0 + rr), __ldg(gr->rc_f1 + rc0 + rr));
+                                const int q = 16 * h + j;
+                                if (b16 + j < R) {
+                                    z[j] = fma(sc ? 0.0 : dcur, s_cf[4 * q + 3], kMagic);
+                                    rec_step(dcur, dprev, sc, cb, *reinterpret_cast<const double2*>(s_cf + 4 * q), s_cf[4 * q + 2]);
                                 } else {
                                     z[j] = kMagic;
                                 }
                             }
-                            store_unit16(A + (r16 >> 4) * 512, kAPlane, z);
+                            if (k < N) store_unit16(A + ((b16 - r0) >> 4) * 512, kAPlane, z);
                         }
                     }
                     tc::fence_proxy_async();
@@ -553,8 +607,11 @@ __global__ void __launch_bounds__(kThreads, 1)
                     cb = gr->cosb[k];
                     dcur = seed_value(nf, gr->pw_sin[(size_t)(it.M - it.Mp) * N + k], gr->pw_cos[(size_t)(it.M + it.Mp) * N + k], sc);
                 }
+                fetch(gr, rc0, rows, M, R, 0);
                 for (int c = 0; c < it.nchunks; ++c, ++g) {
                     const int s = g % kStages, u = g / kStages;
+                    publish();
+                    fetch(gr, rc0, rows, M, R, (c + 1) * kKC);
                     if (!tc::mbar_wait_bounded(&bars[kBarEmpty + s], (uint32_t)((u & 1) ^ 1), kWaitNs, s_abort)) break;
                     unsigned char* A = smem + s * kStageBytes + (m >> 3) * 256 + (m & 7) * 16;
 #pragma unroll 1
@@ -562,10 +619,10 @@ __global__ void __launch_bounds__(kThreads, 1)
                         double z[16];
 #pragma unroll
                         for (int j = 0; j < 16; ++j) {
-                            const int rr = c * kKC + 16 * h + j;
-                            if (rr < it.R) {
-                                z[j] = fma(sc ? 0.0 : dcur, __ldg(&rows[it.M + rr].x), kMagic);
-                                rec_step(dcur, dprev, sc, cb, __ldg(gr->rc_cf + rc0 + rr), __ldg(gr->rc_f1 + rc0 + rr));
+                            const int q = 16 * h + j;
+                            if (c * kKC + q < R) {
+                                z[j] = fma(sc ? 0.0 : dcur, s_cf[4 * q + 3], kMagic);
+                                rec_step(dcur, dprev, sc, cb, *reinterpret_cast<const double2*>(s_cf + 4 * q), s_cf[4 * q + 2]);
                             } else {
                                 z[j] = kMagic;
                             }

@@ -452,6 +452,7 @@ struct FusedArgs {
     int total;               // items of the launch
     long long sync_off;      // double2 offset of the counters in each transform's workspace
     double2* ws;             // single transform: its workspace
+    int discard;             // drop the second pass's input lines from L2 once read (dead workspace)
 };
 
 // Counters of transform z: [0] next item and [1] status (transform 0 only), [2 + c] first-pass
@@ -505,7 +506,7 @@ __global__ void __launch_bounds__(256, Tile::kMinBlocks) fft_fused_kernel(const 
         int* done = fused_sync(f, z) + 2;
         if (pass == 1) {
             if (threadIdx.x == 0) {
-                const volatile int* d = done + c;
+                const volatile int* d = done + c;   // polled; the fence below orders what follows
                 if (*d < T1) {
                     uint64_t t0;
                     asm volatile("mov.u64 %0, %globaltimer;" : "=l"(t0));
@@ -529,11 +530,27 @@ __global__ void __launch_bounds__(256, Tile::kMinBlocks) fft_fused_kernel(const 
         const FftPassArgs& a = f.p[pass];
         const double2* src = a.srcs ? a.srcs[z] : f.src[pass];
         double2* dst = a.dsts ? a.dsts[z] : f.dst[pass];
-        Tile::run(a, c * f.cx[pass] + t % f.cx[pass], t / f.cx[pass], src, dst, smem);
+        const int bx = c * f.cx[pass] + t % f.cx[pass], by = t / f.cx[pass];
+        Tile::run(a, bx, by, src, dst, smem);
         if (pass == 0) {
-            __threadfence();   // this thread's stores, before the count says the tile is done
+            // the CTA's stores are ordered before the barrier; one release by thread 0 publishes
+            // them all (the tile counts as done only after every thread's stores)
             __syncthreads();
-            if (threadIdx.x == 0) atomicAdd(done + c, 1);
+            if (threadIdx.x == 0) {
+                int* d = done + c;
+                asm volatile("red.release.gpu.global.add.s32 [%0], 1;" ::"l"(d) : "memory");
+            }
+        } else if (f.discard) {
+            // the second pass of the inverse read its input (the workspace, dead from here on):
+            // one 128-byte line of kb consecutive layers per element; drop them from L2 so that
+            // the first pass's writes are not written back to HBM
+            __syncthreads();
+            const FftPassArgs& q = f.p[1];
+            for (int e = threadIdx.x; e < q.n; e += blockDim.x) {
+                const double2* line = src + (long long)bx * q.kb * q.src.sv + (long long)by * q.src.sb + (long long)e * q.src.se;
+                if ((reinterpret_cast<uintptr_t>(line) & 127) == 0)   // whole lines only
+                    asm volatile("discard.global.L2 [%0], 128;" ::"l"(line) : "memory");
+            }
         }
     }
 }
@@ -676,10 +693,10 @@ cudaError_t fft_pass_launch(const double2* src, double2* dst, const FftPassArgs&
     return cudaGetLastError();
 }
 
-// Fused-pass choice per transform length (index n <= 1024; default on), set by the autotuner.
+// Fused-pass choice per transform length (index n <= 1024; default off), set by the autotuner.
 constexpr int kFusedMaxN = 1024;
 signed char g_fft_fused[kFusedMaxN + 1] = {};   // 0 default (on), 1 on, -1 off
-bool g_fft_fused_all = true;
+bool g_fft_fused_all = false;
 bool fft_fused_enabled(int n)
 {
     if (n >= 0 && n <= kFusedMaxN && g_fft_fused[n]) return g_fft_fused[n] > 0;
@@ -738,6 +755,9 @@ cudaError_t fft_fused_launch(int sign, const FftPassArgs& p0, const FftPassArgs&
     f.total = f.per_z * nz;
     f.sync_off = sync_off;
     f.ws = ws;
+    // inverse (I2 in place, then I1 out of the workspace): the workspace is dead once I1 has read
+    // it; its lines can be dropped when one tile's kb layers fill whole 128-byte lines
+    f.discard = (sign > 0 && p1.src.sv == 1 && p1.kb * (int)sizeof(double2) == 128 && p1.dst.sv != 1) ? 1 : 0;
     fused_sync_clear<<<nz, 128, 0, stream>>>(f, 2 + f.nchunks);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;

@@ -50,7 +50,7 @@ size_t fft_pass_smem_bytes(const FftPassArgs& a);
 // when the passes cannot be fused (fft_fused_chunk == 0).
 constexpr int kFftSyncBytes = 4096;
 int fft_fused_chunk(const FftPassArgs& p0, const FftPassArgs& p1);
-// Whether transforms of length n use the fused launch (default on; pfsoft_tune_fft_fused sets it
+// Whether transforms of length n use the fused launch (default off; pfsoft_tune_fft_fused sets it
 // per length, or for every length with n <= 0).
 bool fft_fused_enabled(int n);
 void fft_set_fused(int n, int on);

@@ -37,7 +37,7 @@ def test_fused_equals_two_passes(lib, B):
         assert lib.pfsoft_tune_fft_fused(0, 1) == 0
         g1, f1 = _round_trip(lib, B, c)
     finally:
-        lib.pfsoft_tune_fft_fused(0, 1)
+        lib.pfsoft_tune_fft_fused(0, 0)   # the library default
     assert torch.equal(g1, g2), f"B={B}: iDSOFT grids differ"
     assert torch.equal(f1, f2), f"B={B}: DSOFT coefficients differ"
     assert (torch.linalg.vector_norm(f1 - c) / torch.linalg.vector_norm(c)).item() <= 1e-13
@@ -67,7 +67,7 @@ def test_fused_batch_equals_two_passes(lib, split):
             lib.pfsoft_batch_destroy(plan)
             out[fused] = (gs, fs)
     finally:
-        lib.pfsoft_tune_fft_fused(0, 1)
+        lib.pfsoft_tune_fft_fused(0, 0)   # the library default
     for i, B in enumerate(bws):
         assert torch.equal(out[0][0][i], out[1][0][i]), f"B={B}: grids differ"
         assert torch.equal(out[0][1][i], out[1][1][i]), f"B={B}: coefficients differ"

@@ -151,6 +151,7 @@ def test_split_server_mixed_bandwidths(lib, oracle):
             srv.submit(direction, B, inp, o).wait()
             alone.append(o)
         srv.pause()
+        srv.reset_stats()
         together, reqs = [], []
         for direction, B, inp, _ in mix:
             o = _out_like(torch, direction, B)
