@@ -11,10 +11,13 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <algorithm>
 #include <atomic>
+#include <condition_variable>
 #include <map>
 #include <mutex>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "../../include/pfsoft_b200.h"
@@ -56,7 +59,165 @@ struct StagingContext {
     void* h_ws = nullptr;
     size_t h_grid_bytes = 0, h_coef_bytes = 0, h_ws_bytes = 0;
     cudaStream_t h_stream = nullptr;
+    // pageable host buffers go through two pinned bounce chunks (allocated on first use)
+    void* bounce[2] = {nullptr, nullptr};
+    cudaEvent_t bounce_ev[2] = {nullptr, nullptr};
 };
+
+constexpr size_t kBounceBytes = (size_t)16 << 20;
+
+// Host threads that copy the slices of one large memcpy in parallel (the pageable side of a
+// bounce-buffer transfer is a host memory copy, which one thread does at a fraction of the
+// host's memory bandwidth). The calling thread takes a slice too.
+class CopyPool {
+  public:
+    static CopyPool& get()
+    {
+        static CopyPool* p = new CopyPool();   // lives until process exit
+        return *p;
+    }
+
+    void copy(void* dst, const void* src, size_t bytes)
+    {
+        const int parts = (int)std::min<size_t>((size_t)nthreads_ + 1, std::max<size_t>(1, bytes >> 20));
+        if (parts <= 1) {
+            std::memcpy(dst, src, bytes);
+            return;
+        }
+        std::unique_lock<std::mutex> call(call_mu_);   // one parallel copy at a time
+        const size_t slice = (bytes + parts - 1) / parts;
+        {
+            std::lock_guard<std::mutex> lk(mu_);
+            dst_ = static_cast<char*>(dst);
+            src_ = static_cast<const char*>(src);
+            bytes_ = bytes;
+            slice_ = slice;
+            next_ = 1;
+            parts_ = parts;
+            pending_ = parts - 1;
+            ++gen_;
+        }
+        cv_.notify_all();
+        std::memcpy(dst, src, std::min(slice, bytes));   // slice 0 on the calling thread
+        std::unique_lock<std::mutex> lk(mu_);
+        done_cv_.wait(lk, [&] { return pending_ == 0; });
+    }
+
+  private:
+    CopyPool()
+    {
+        const unsigned hw = std::thread::hardware_concurrency();
+        nthreads_ = (int)std::max(1u, std::min(7u, hw > 1 ? hw - 1 : 1u));
+        for (int i = 0; i < nthreads_; ++i) std::thread([this] { run(); }).detach();
+    }
+
+    void run()
+    {
+        unsigned long long seen = 0;
+        std::unique_lock<std::mutex> lk(mu_);
+        for (;;) {
+            cv_.wait(lk, [&] { return gen_ != seen && next_ < parts_; });
+            while (next_ < parts_) {
+                const int part = next_++;
+                const size_t off = (size_t)part * slice_;
+                const size_t n = off < bytes_ ? std::min(slice_, bytes_ - off) : 0;
+                char* d = dst_ + off;
+                const char* sp = src_ + off;
+                lk.unlock();
+                if (n) std::memcpy(d, sp, n);
+                lk.lock();
+                if (--pending_ == 0) done_cv_.notify_all();
+            }
+            seen = gen_;
+        }
+    }
+
+    int nthreads_ = 1;
+    std::mutex call_mu_, mu_;
+    std::condition_variable cv_, done_cv_;
+    char* dst_ = nullptr;
+    const char* src_ = nullptr;
+    size_t bytes_ = 0, slice_ = 0;
+    int next_ = 0, parts_ = 0, pending_ = 0;
+    unsigned long long gen_ = 0;
+};
+
+bool is_pinned(const void* p)
+{
+    cudaPointerAttributes a;
+    if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    return a.type == cudaMemoryTypeHost;
+}
+
+cudaError_t bounce_ready(StagingContext* st)
+{
+    for (int b = 0; b < 2; ++b) {
+        if (!st->bounce[b]) {
+            cudaError_t e = cudaHostAlloc(&st->bounce[b], kBounceBytes, cudaHostAllocDefault);
+            if (e != cudaSuccess) return e;
+        }
+        if (!st->bounce_ev[b]) {
+            cudaError_t e = cudaEventCreateWithFlags(&st->bounce_ev[b], cudaEventDisableTiming);
+            if (e != cudaSuccess) return e;
+        }
+    }
+    return cudaSuccess;
+}
+
+// Host-to-device copy, stream ordered: pinned sources go straight to DMA; pageable ones are
+// copied by the host threads into the two pinned chunks in turn while the previous chunk's DMA runs.
+cudaError_t copy_in(StagingContext* st, void* dev, const void* host, size_t bytes, cudaStream_t s)
+{
+    if (is_pinned(host)) return cudaMemcpyAsync(dev, host, bytes, cudaMemcpyHostToDevice, s);
+    cudaError_t e = bounce_ready(st);
+    bool used[2] = {false, false};
+    for (size_t off = 0, i = 0; e == cudaSuccess && off < bytes; off += kBounceBytes, ++i) {
+        const int b = (int)(i & 1);
+        const size_t n = std::min(kBounceBytes, bytes - off);
+        if (used[b]) e = cudaEventSynchronize(st->bounce_ev[b]);   // its last DMA has read it
+        if (e != cudaSuccess) break;
+        CopyPool::get().copy(st->bounce[b], static_cast<const char*>(host) + off, n);
+        e = cudaMemcpyAsync(static_cast<char*>(dev) + off, st->bounce[b], n, cudaMemcpyHostToDevice, s);
+        if (e == cudaSuccess) e = cudaEventRecord(st->bounce_ev[b], s);
+        used[b] = true;
+    }
+    return e;
+}
+
+// Device-to-host copy after the work queued on s; returns when the host buffer holds the data.
+// Pageable destinations: chunk i's DMA into one pinned chunk overlaps the host threads' copy of
+// chunk i-1 out of the other.
+cudaError_t copy_out(StagingContext* st, void* host, const void* dev, size_t bytes, cudaStream_t s)
+{
+    if (is_pinned(host)) {
+        cudaError_t e = cudaMemcpyAsync(host, dev, bytes, cudaMemcpyDeviceToHost, s);
+        return e == cudaSuccess ? cudaStreamSynchronize(s) : e;
+    }
+    cudaError_t e = bounce_ready(st);
+    size_t prev_off = 0, prev_n = 0;
+    int prev_b = -1;
+    for (size_t off = 0, i = 0; e == cudaSuccess && off < bytes; off += kBounceBytes, ++i) {
+        const int b = (int)(i & 1);
+        const size_t n = std::min(kBounceBytes, bytes - off);
+        e = cudaMemcpyAsync(st->bounce[b], static_cast<const char*>(dev) + off, n, cudaMemcpyDeviceToHost, s);
+        if (e == cudaSuccess) e = cudaEventRecord(st->bounce_ev[b], s);
+        if (e == cudaSuccess && prev_b >= 0) {
+            e = cudaEventSynchronize(st->bounce_ev[prev_b]);
+            if (e == cudaSuccess) CopyPool::get().copy(static_cast<char*>(host) + prev_off, st->bounce[prev_b], prev_n);
+        }
+        prev_b = b;
+        prev_off = off;
+        prev_n = n;
+    }
+    if (e == cudaSuccess && prev_b >= 0) {
+        e = cudaEventSynchronize(st->bounce_ev[prev_b]);
+        if (e == cudaSuccess) CopyPool::get().copy(static_cast<char*>(host) + prev_off, st->bounce[prev_b], prev_n);
+    }
+    return e;
+}
 
 struct DeviceState {
     std::mutex mu;
@@ -494,15 +655,15 @@ static int host_staged(int B, bool forward, const double* in, double* out)
     cudaStream_t s = st->h_stream;
     int rc;
     if (forward) {
-        PF_CUDA(cudaMemcpyAsync(st->h_grid, in, gb, cudaMemcpyHostToDevice, s));
+        PF_CUDA(copy_in(st, st->h_grid, in, gb, s));
         rc = run_dsoft(static_cast<const double*>(st->h_grid), B, static_cast<double*>(st->h_coef), st->h_ws, s);
         if (rc) return rc;
-        PF_CUDA(cudaMemcpyAsync(out, st->h_coef, cb, cudaMemcpyDeviceToHost, s));
+        PF_CUDA(copy_out(st, out, st->h_coef, cb, s));
     } else {
-        PF_CUDA(cudaMemcpyAsync(st->h_coef, in, cb, cudaMemcpyHostToDevice, s));
+        PF_CUDA(copy_in(st, st->h_coef, in, cb, s));
         rc = run_idsoft(static_cast<const double*>(st->h_coef), B, static_cast<double*>(st->h_grid), st->h_ws, s);
         if (rc) return rc;
-        PF_CUDA(cudaMemcpyAsync(out, st->h_grid, gb, cudaMemcpyDeviceToHost, s));
+        PF_CUDA(copy_out(st, out, st->h_grid, gb, s));
     }
     PF_CUDA(cudaStreamSynchronize(s));
     return PFSOFT_OK;

@@ -171,6 +171,20 @@ def test_host_staged_matches_device(lib):
     np.testing.assert_array_equal(f_host, gpu_dsoft(lib, g_host, B)[0])
 
 
+def test_host_staged_pageable_large_matches_device(lib):
+    """B = 96 (a 221 MB grid: the pageable copies go through the pinned bounce chunks, 16 MB
+    each, in several rounds) on numpy (pageable) buffers, against the device entry points."""
+    B = 96
+    c = orc.coeffs_uniform(B, seed=9)
+    N = 2 * B
+    g_host = np.empty((N, N, N), dtype=np.complex128)
+    assert lib.pfsoft_idsoft_host(c.ctypes.data, B, g_host.ctypes.data) == 0, lib.pfsoft_last_error()
+    np.testing.assert_array_equal(g_host, gpu_idsoft(lib, c, B))
+    f_host = np.empty_like(c)
+    assert lib.pfsoft_dsoft_host(g_host.ctypes.data, B, f_host.ctypes.data) == 0, lib.pfsoft_last_error()
+    np.testing.assert_array_equal(f_host, gpu_dsoft(lib, g_host, B)[0])
+
+
 @pytest.mark.parametrize("cols,rows,lays", [(8, 8, 3), (32, 32, 5), (24, 40, 2), (7, 9, 3), (256, 256, 2), (512, 512, 1),
                                              (512, 384, 5), (384, 512, 6), (96, 192, 3), (192, 96, 2),
                                              (32, 96, 4)])
