@@ -252,6 +252,64 @@ def _timed(fn, steps, warmup):
     return e0.elapsed_time(e1) / steps
 
 
+def pinned_copy_floor(nbytes: int, steps: int) -> dict:
+    """What the host link gives with no transform: per step `nbytes` host-to-device and `nbytes`
+    device-to-host, each one cudaMemcpyAsync on its own stream so the two directions overlap,
+    pinned host memory; wall clock over `steps` steps, in the headline's unit (2 transforms a step)."""
+    import torch
+    hin = torch.empty(nbytes, dtype=torch.uint8).pin_memory()
+    hout = torch.empty(nbytes, dtype=torch.uint8).pin_memory()
+    din = torch.empty(nbytes, dtype=torch.uint8, device="cuda")
+    dout = torch.empty(nbytes, dtype=torch.uint8, device="cuda")
+    s1, s2 = torch.cuda.Stream(), torch.cuda.Stream()
+
+    def step():
+        with torch.cuda.stream(s1):
+            din.copy_(hin, non_blocking=True)
+        with torch.cuda.stream(s2):
+            hout.copy_(dout, non_blocking=True)
+
+    step()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        step()
+    torch.cuda.synchronize()
+    sec = time.perf_counter() - t0
+    del hin, hout, din, dout
+    return {"value": TRANSFORMS_PER_STEP * steps / sec, "unit": UNIT, "steps": steps,
+            "gb_per_s_each_way": nbytes * steps / sec / 1e9,
+            "what": f"{nbytes} bytes host-to-device and {nbytes} device-to-host per step, two streams, pinned"}
+
+
+def dropin_cpp_timing(bandwidth: int, steps: int) -> dict:
+    """Transforms/s of the C++ drop-in header's FourierTransforms::IDSOFT + DSOFT on the header's own
+    pageable containers (tests/cpp/dropin_timing.cpp, compiled here against the library)."""
+    try:
+        import shutil
+        import pfsoftlib_b200
+        pfsoftlib_b200.load()
+        libdir = os.path.join(ROOT, "pfsoftlib_b200")
+        cxx = "/usr/bin/g++" if os.path.exists("/usr/bin/g++") else shutil.which("g++")
+        with tempfile.TemporaryDirectory() as td:
+            exe = os.path.join(td, "dropin_timing")
+            subprocess.run([cxx, "-std=c++17", "-O2", "-I", os.path.join(ROOT, "include"),
+                            os.path.join(ROOT, "tests", "cpp", "dropin_timing.cpp"), "-o", exe,
+                            "-L", libdir, "-lpfsoft_b200", f"-Wl,-rpath,{libdir}"],
+                           check=True, capture_output=True, text=True, timeout=300)
+            r = subprocess.run([exe, str(bandwidth), str(steps), "1"], capture_output=True, text=True,
+                               timeout=600)
+        out = json.loads(r.stdout.strip().splitlines()[-1])
+        if r.returncode != 0:
+            out["error"] = f"exit {r.returncode}"
+        return {"value": out["transforms_per_s"], "unit": UNIT, "steps": steps,
+                "max_abs_err": out["max_abs_err"], "ok": r.returncode == 0,
+                "api": "pfsoft::FourierTransforms::IDSOFT + DSOFT (include/pfsoft_b200/pfsoft.hpp) on "
+                       "grid3D / DSOFTFourierCoefficients storage (pageable new[])"}
+    except Exception as exc:   # reported, the headline line still prints
+        return {"error": f"{type(exc).__name__}: {exc}"[:300]}
+
+
 class _Plan:
     """A batch plan over device tensors (pfsoft_batch_*)."""
 
@@ -946,6 +1004,14 @@ def main():
                     "h2d_bytes_per_step": COEF_BYTES + GRID_BYTES, "d2h_bytes_per_step": GRID_BYTES + COEF_BYTES,
                     "api": "pfsoft_idsoft_host + pfsoft_dsoft_host on pageable numpy buffers"}
     del chp, ghp, fhp
+    # the copy floor of e2e: the same bytes moved by plain pinned copies, host-to-device and
+    # device-to-host on two streams at once (what the link gives with no transform at all)
+    copy_floor = pinned_copy_floor(COEF_BYTES + GRID_BYTES, e2e_steps)
+    e2e["copy_floor"] = copy_floor
+    e2e["frac_of_copy_floor"] = e2e["value"] / copy_floor["value"]
+    # the C++ drop-in itself: FourierTransforms::IDSOFT / DSOFT of pfsoft_b200/pfsoft.hpp on its
+    # own containers (pageable new[] storage), a compiled program timed by its own clock
+    e2e_dropin = dropin_cpp_timing(B, e2e_steps) if rank == 0 else None
 
     # ---- CPU baseline (rank 0, N = 1 only)
     cpu = None
@@ -970,7 +1036,7 @@ def main():
         "warmup": max(3, args.warmup), "ms_per_step": ms / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "config": workload_config(),
-        "e2e": e2e, "e2e_sequential": e2e_sequential, "e2e_pageable": e2e_pageable,
+        "e2e": e2e, "e2e_sequential": e2e_sequential, "e2e_pageable": e2e_pageable, "e2e_dropin_cpp": e2e_dropin,
         "gpu_launches": int(launches), "roofline": roofline,
         "stages": stages, "cpu_baseline": cpu, "accuracy": acc, "clocks": clk,
         "parallelism": f"replicas x{world} (independent transforms per GPU, no collective)",

@@ -15,17 +15,19 @@ def _cxx():
     return "/usr/bin/g++" if os.path.exists("/usr/bin/g++") else shutil.which("g++")
 
 
-def _build(out):
+def _build(out, src=SRC):
     import pfsoftlib_b200
 
     pfsoftlib_b200.load()   # builds libpfsoft_b200.so if needed
-    cmd = [_cxx(), "-std=c++17", "-O2", "-Wall", "-I", os.path.join(ROOT, "include"), SRC, "-o", out,
+    cmd = [_cxx(), "-std=c++17", "-O2", "-Wall", "-I", os.path.join(ROOT, "include"), src, "-o", out,
            "-L", LIBDIR, "-lpfsoft_b200", f"-Wl,-rpath,{LIBDIR}"]
     subprocess.run(cmd, check=True, capture_output=True, text=True)
 
 
 def test_header_compiles(tmp_path):
     _build(str(tmp_path / "roundtrip"))
+    # the drop-in timing program the benchmark runs
+    _build(str(tmp_path / "dropin_timing"), os.path.join(ROOT, "tests", "cpp", "dropin_timing.cpp"))
 
 
 @pytest.mark.gpu
