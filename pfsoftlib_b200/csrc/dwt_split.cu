@@ -15,8 +15,8 @@
 // the generated operand times the concatenated planes 0..5-s of the data operand lands in
 // accumulator planes s..5 (significance e = s + t; the 15 products with e > 5 are dropped). A
 // plane product summed over any K <= 2^16 is exact, so every bandwidth up to 256 (K = 512) is
-// exact in the integer sums; the epilogue combines the six planes in FP64 (Horner in 2^-8,
-// smallest first) and undoes the scales. FP64 stays for the seeds, the recurrence, the weights
+// exact in the integer sums; the epilogue combines the six planes (two 64-bit integer partial
+// sums, then FP64) and undoes the scales. FP64 stays for the seeds, the recurrence, the weights
 // and that final sum.
 //
 // Work items, dealt to the persistent CTAs in snake order over one index space:
@@ -27,26 +27,37 @@
 // The items are not listed: a launch gets one segment per bandwidth group (host:
 // dwt_split_segments, largest bandwidth first), and item i of a segment is class i / (pairs *
 // tiles) -- classes run longest first (M ascending) -- then transform pair, then tile.
+//
+// The data operand reaches shared memory by untiled bulk copies (cp.async.bulk, completion on an
+// mbarrier), never by per-thread gathers: forward, the chunk's 32 beta of each case's bin column
+// (contiguous in the spectrum); inverse, a class-major copy of the scaled coefficients that
+// split_inv_prepare_kernel writes once per launch (the packed coefficient layout scatters a
+// class's degrees over the whole array). Each copy also brings the columns' scale entries.
 // One CTA of 12 warps per SM, roles fixed per warp:
 //   warp 0      issues the MMAs (one lane) into one of two accumulator sets in tensor memory;
-//   warps 1-3   loaders: the data operand of a chunk (spectrum bins or coefficients) to digit planes;
+//   warp 1      issues the bulk copies of each chunk's data into a ring of raw slots;
+//   warps 2-3   digitise a chunk's raw data (alternate chunks) into the stage's B operand;
 //   warps 4-7   epilogue: read an accumulator set back (warp w reads lanes 32(w%4) ..), combine, store;
 //   warps 8-11  generators: the Wigner rows of a chunk to digit planes (forward: one warp per
 //               chunk of 32 beta columns, all rows; inverse: the four warps on the tile's 128 beta
 //               columns, 32 degrees per chunk).
 // Chunks move through a ring of shared-memory stages (full / empty mbarriers; empty is signalled by
-// tcgen05.commit), accumulator sets through accfull / accempty, so generation, loading, MMAs and the
-// epilogue of different chunks and items overlap. Every wait is bounded (%globaltimer); a wait that
-// runs out sets a CTA-wide abort flag, every role leaves, the MMA lane waits (bounded) for its
-// committed MMAs before the tensor memory is freed, and *status is set to 1.
+// tcgen05.commit) and raw slots (rawfull by the copies' byte count, rawempty by the digitising
+// warp), accumulator sets through accfull / accempty, so copies, generation, digitisation, MMAs and
+// the epilogue of different chunks and items overlap. Every wait is bounded (%globaltimer); a wait
+// that runs out sets a CTA-wide abort flag, every role leaves, the copy warp waits (bounded) for
+// its copies in flight and the MMA lane for its committed MMAs before the CTA ends, and *status is
+// set to 1.
 //
 // Operand layouts in shared memory (no swizzle; see tc_sm100.cuh), per stage and plane:
 //   A forward (MN-major, rows = degrees):  (r/16)*512 + (k/8)*128 + (k%8)*16 + (r%16)
 //   A inverse (K-major, rows = beta):      (m/8)*256 + (j/16)*128 + (m%8)*16 + (j%16)
-//   B both    (K-major, rows = columns):   (n/8)*256 + (k/16)*128 + (n%8)*16 + (k%16),
-//             plane t of the data operand at rows 16*nt*t .. (planes concatenated along N)
-// so that a generator lane writes whole 16-byte units of 16 consecutive degrees of its beta column,
-// and a loader lane 8-byte halves of 8 consecutive K of one column.
+//   B both    (K-major): transform t at t*3072, plane p at +p*512, row n = 2 case + (re, im):
+//             (n/8)*256 + (k/16)*128 + (n%8)*16 + (k%16)  -- a transform's planes are contiguous,
+//             so planes 0..5-s of one transform are one B operand of N = 16 (6 - s) rows.
+// The generator inner loops carry no data-dependent branch: rows past the class's last degree
+// get zero recurrence coefficients and a zero row scale (digits 0), and a column still scaled by
+// 2^600 (tiny seed, see dwt.cu) is checked for its rescale once per 16 degrees.
 
 #include <algorithm>
 #include <cstdint>
@@ -60,6 +71,20 @@
 
 namespace pfsoft_dev {
 
+// Chunks of 32 degrees the inverse operand of classes 0 .. (M, M')-1 occupies (class-major copy):
+// sum over m < M of (m + 1) ceil((B - m) / 32), plus M' ceil((B - M) / 32). ceil((B - m) / 32) = v
+// for m in [B - 32v, B - 32(v - 1) - 1], so the sum runs over at most eight blocks.
+__host__ __device__ __forceinline__ long long inv_chunk_prefix(int B, int M, int Mp)
+{
+    long long s = 0;
+    for (int v = 1; 32 * (v - 1) < B; ++v) {
+        const int lo = B - 32 * v > 0 ? B - 32 * v : 0;
+        const int hi = (M - 1) < (B - 32 * (v - 1) - 1) ? (M - 1) : (B - 32 * (v - 1) - 1);
+        if (hi >= lo) s += (long long)v * ((long long)(lo + hi + 2) * (hi - lo + 1) / 2);
+    }
+    return s + (long long)Mp * ((B - M + 31) / 32);
+}
+
 namespace {
 
 using namespace dwtk;
@@ -68,30 +93,46 @@ constexpr int kNT = 2;                 // transforms per work item (at most)
 constexpr int kPlanes = 6;             // digits per operand
 constexpr int kKC = 32;                // K per chunk: one kind::i8 MMA
 constexpr int kStages = 6;             // operand ring
+constexpr int kRaw = 4;                // raw-data ring
 constexpr int kAccSets = 2;
 constexpr int kAccStride = 256;        // tensor-memory columns between the two accumulator sets
+constexpr int kAccT = 16 * kPlanes;    // accumulator columns per transform: 6 planes x 16
 constexpr uint32_t kTmemCols = 512;
 constexpr int kThreads = 384;
-constexpr int kLoadWarp0 = 1, kLoadWarps = 3;
+constexpr int kCopyWarp = 1;
+constexpr int kConvWarp0 = 2, kConvWarps = 2;
 constexpr int kEpiWarp0 = 4;
 constexpr int kGenWarp0 = 8, kGenWarps = 4;
 constexpr uint64_t kWaitNs = 2000000000ull;   // 2 s
 
 constexpr int kAPlane = 4096;                       // 128 rows x 32 bytes of K
 constexpr int kABytes = kPlanes * kAPlane;          // 24 KB
-constexpr int kBRows = 16 * kNT * kPlanes;          // 192
-constexpr int kBBytes = kBRows / 8 * 256;           // 6 KB
+constexpr int kBPlane = 512;                        // 16 rows x 32 bytes of K
+constexpr int kBT = kPlanes * kBPlane;              // one transform's planes: 3 KB
+constexpr int kBBytes = kNT * kBT;                  // 6 KB
 constexpr int kStageBytes = kABytes + kBBytes;
-constexpr int kOffCoef = kStages * kStageBytes;     // generators: 32 steps x {c1, f1 f2, f1, row scale} per warp
-constexpr int kOffBar = kOffCoef + kGenWarps * 32 * 4 * 8;
-// mbarriers: full[kStages], empty[kStages], accfull[2], accempty[2], drain, never (test knob)
+// raw slot, per transform: 8 scale entries {cs47 re, im}, {1/scale re, im} (256 B), then the 8
+// cases' 32 double2 each at a 528-byte pitch (a quarter warp reading one value of each case hits
+// eight distinct bank groups)
+constexpr int kRawHdr = 256;
+constexpr int kRawPitch = 528;
+constexpr int kRawT = kRawHdr + 8 * kRawPitch;      // 4480
+constexpr int kRawBytes = kNT * kRawT;
+constexpr int kOffRaw = kStages * kStageBytes;
+constexpr int kOffCoef = kOffRaw + kRaw * kRawBytes;   // generators: 32 steps x {c1, f1 f2, f1, row scale} per warp
+constexpr int kOffEpi = kOffCoef + kGenWarps * 32 * 4 * 8;   // epilogue: 16 x {1/scale re, im} per warp
+constexpr int kOffBar = kOffEpi + 4 * 16 * 16;
+// mbarriers: full[kStages], empty[kStages], accfull[2], accempty[2], rawfull[kRaw], rawempty[kRaw],
+// drain, never (test knob)
 constexpr int kBarFull = 0, kBarEmpty = kStages, kBarAccFull = 2 * kStages, kBarAccEmpty = 2 * kStages + kAccSets,
-              kBarDrain = 2 * kStages + 2 * kAccSets, kBarNever = kBarDrain + 1, kNumBars = kBarNever + 1;
+              kBarRawFull = 2 * kStages + 2 * kAccSets, kBarRawEmpty = kBarRawFull + kRaw,
+              kBarDrain = kBarRawEmpty + kRaw, kBarNever = kBarDrain + 1, kNumBars = kBarNever + 1;
 constexpr int kOffMisc = kOffBar + kNumBars * 8;    // tensor-memory address, abort flag
 constexpr int kSmemBytes = kOffMisc + 16;
 static_assert(kStageBytes % 1024 == 0, "stages stay 1 KB aligned");
+static_assert(kRawT % 16 == 0 && kRawPitch % 16 == 0 && kOffRaw % 16 == 0, "bulk-copy destinations 16-byte aligned");
 static_assert(kSmemBytes <= 227 * 1024, "shared memory");
-static_assert(16 * kNT * kPlanes <= kAccStride, "an accumulator set fits its column range");
+static_assert(kNT * kAccT <= kAccStride, "an accumulator set fits its column range");
 
 constexpr double kTwo47 = 140737488355328.0;        // 2^47
 // 2^52 + sum_{i<6} 128 * 256^i: adding it to x * 2^47 (|x| < 0.5) leaves round(x * 2^47) + C in
@@ -103,6 +144,12 @@ constexpr double kMagic = 4503599627370496.0 + 141289400074368.0;
 struct SplitSeg {
     int group, first, count, pairs, tiles, T, pad0, pad1;
 };
+
+// Operand area past each transform's spectrum (double2 offsets from X + N^3): the column scale
+// table (two double2 per (class, case)), the row table (one per degree), the inverse operand in
+// class-major order (256 double2 per 32-degree chunk: 8 cases x 32 degrees).
+__host__ __device__ __forceinline__ size_t aux_rows(int B) { return (size_t)16 * num_classes(B); }
+__host__ __device__ __forceinline__ size_t aux_inv(int B) { return aux_rows(B) + (size_t)B; }
 
 // Digit words of four magic-biased values: w[p] holds byte (5 - p) of each value (value i in
 // byte i), XOR 0x80, i.e. plane p of the signed digits, most significant plane first.
@@ -206,27 +253,52 @@ __device__ __forceinline__ int cta_item(int r, int n_items)
     return i < n_items ? i : -1;
 }
 
-// Row table of a transform's operand-scale area: {scale * 2^47, 1 / scale} per degree l.
-__device__ __forceinline__ const double2* row_table(const DwtGroup* gr, int t)
+__device__ __forceinline__ const double2* aux_of(const DwtGroup* gr, int t)
 {
-    const int N = gr->N, B = gr->B;
-    const size_t a0 = (size_t)N * N > (size_t)8 * num_classes(B) ? (size_t)N * N : (size_t)8 * num_classes(B);
-    return gr->X[t] + (size_t)N * N * N + a0;
+    const size_t N = (size_t)gr->N;
+    return gr->X[t] + N * N * N;
 }
 
-// One recurrence step of a beta column (fn_dwt.hpp:167-199): d(l+1) = d(l)(f1 f2 + f1 cos b) + c1 d(l-1);
-// a column whose seed was scaled by 2^600 rescales once it grows past 2^300 (and stores 0 meanwhile).
-__device__ __forceinline__ void rec_step(double& dcur, double& dprev, int& sc, double cb, double2 cf, double f1)
+// One recurrence step of a beta column (fn_dwt.hpp:167-199): d(l+1) = d(l)(f1 f2 + f1 cos b) + c1 d(l-1).
+__device__ __forceinline__ void rec_step(double& dcur, double& dprev, double cb, double2 cf, double f1)
 {
     const double t = fma(f1, cb, cf.y);
     const double u = cf.x * dprev;
     const double nx = fma(dcur, t, u);
     dprev = dcur;
     dcur = nx;
+}
+
+// A column whose seed was scaled by 2^600 rescales once it has grown past 2^300 (it stores 0 while
+// scaled: its true magnitude is below 2^-300). Checked every 16 degrees.
+__device__ __forceinline__ void rescale_check(double& dcur, double& dprev, int& sc)
+{
     if (sc && fabs(dcur) >= 0x1p300) {
         dcur *= 0x1p-600;
         dprev *= 0x1p-600;
         --sc;
+    }
+}
+
+// 16 recurrence steps of the lane's column from the staged coefficients s_cf[4 q + {0..3}]
+// (q = q0 .. q0+15), writing the magic-biased digits of the current row before each step.
+__device__ __forceinline__ void gen16(double (&z)[16], double& dcur, double& dprev, int sc, double cb,
+                                      const double* s_cf, int q0)
+{
+#pragma unroll
+    for (int j = 0; j < 16; ++j) {
+        const int q = q0 + j;
+        z[j] = fma(sc ? 0.0 : dcur, s_cf[4 * q + 3], kMagic);
+        rec_step(dcur, dprev, cb, *reinterpret_cast<const double2*>(s_cf + 4 * q), s_cf[4 * q + 2]);
+    }
+}
+
+__device__ __forceinline__ void adv16(double& dcur, double& dprev, double cb, const double* s_cf, int q0)
+{
+#pragma unroll
+    for (int j = 0; j < 16; ++j) {
+        const int q = q0 + j;
+        rec_step(dcur, dprev, cb, *reinterpret_cast<const double2*>(s_cf + 4 * q), s_cf[4 * q + 2]);
     }
 }
 
@@ -247,12 +319,16 @@ __global__ void __launch_bounds__(kThreads, 1)
     }
     if (tid == 32) {
         for (int s = 0; s < kStages; ++s) {
-            tc::mbar_init(&bars[kBarFull + s], DIR == 0 ? 2 : 1 + kGenWarps);   // generator warp(s) + loader warp
+            tc::mbar_init(&bars[kBarFull + s], DIR == 0 ? 2 : 1 + kGenWarps);   // generator warp(s) + digitising warp
             tc::mbar_init(&bars[kBarEmpty + s], 1);                           // tcgen05.commit
         }
         for (int a = 0; a < kAccSets; ++a) {
             tc::mbar_init(&bars[kBarAccFull + a], 1);
             tc::mbar_init(&bars[kBarAccEmpty + a], 4);   // the four epilogue warps
+        }
+        for (int r = 0; r < kRaw; ++r) {
+            tc::mbar_init(&bars[kBarRawFull + r], 1);    // arrive.expect_tx of the copy warp + the bytes
+            tc::mbar_init(&bars[kBarRawEmpty + r], 1);   // the digitising warp
         }
         tc::mbar_init(&bars[kBarDrain], 1);
         tc::mbar_init(&bars[kBarNever], 1);
@@ -283,7 +359,6 @@ __global__ void __launch_bounds__(kThreads, 1)
             }
             tc::fence_after_sync();
             const uint32_t dbase = tmem + (uint32_t)(a * kAccStride);
-            const int cols = 16 * it.nt;
             for (int c = 0; c < it.nchunks; ++c, ++g) {
                 const int s = g % kStages, u = g / kStages;
                 if (!tc::mbar_wait_bounded(&bars[kBarFull + s], (uint32_t)(u & 1), kWaitNs, s_abort)) {
@@ -293,12 +368,13 @@ __global__ void __launch_bounds__(kThreads, 1)
                 tc::fence_after_sync();
                 if (lane == 0) {
                     const uint32_t a0 = smem_base + s * kStageBytes, b0 = a0 + kABytes;
-                    const uint64_t bd = tc::sdesc(b0, 128, 256);
 #pragma unroll
                     for (int p = 0; p < kPlanes; ++p) {
                         const uint64_t ad = DIR == 0 ? tc::sdesc(a0 + p * kAPlane, 128, 512) : tc::sdesc(a0 + p * kAPlane, 128, 256);
-                        tc::mma_s8(dbase + (uint32_t)(cols * p), ad, bd, tc::idesc_s8(128, cols * (kPlanes - p), DIR == 0, false),
-                                   !(c == 0 && p == 0));
+                        const uint32_t id = tc::idesc_s8(128, 16 * (kPlanes - p), DIR == 0, false);
+                        for (int t = 0; t < it.nt; ++t)
+                            tc::mma_s8(dbase + (uint32_t)(kAccT * t + 16 * p), ad, tc::sdesc(b0 + t * kBT, 128, 256), id,
+                                       !(c == 0 && p == 0));
                     }
                     tc::mma_commit(&bars[kBarEmpty + s]);
                 }
@@ -316,206 +392,215 @@ __global__ void __launch_bounds__(kThreads, 1)
                 if (tc::globaltimer_ns() - t0 > kWaitNs) break;
         }
         __syncwarp();
-    } else if (warp >= kLoadWarp0 && warp < kLoadWarp0 + kLoadWarps) {
-        // ------------------------------------------------------------------ loaders (data operand)
-        const int L = warp - kLoadWarp0;
+    } else if (warp == kCopyWarp) {
+        // ------------------------------------------------------------------ bulk copies (data operand)
+        // lane i < 9 nt: transform i / 9, entry j = i % 9: j < 8 the 32 values of case j, j = 8 the
+        // transform's 8 scale entries
         int g = 0;
         for (int r = 0;; ++r) {
             const int idx = cta_item(r, n_items);
             if (idx < 0 || *s_abort) break;
             const ItemGeo it = item_geo<DIR>(groups, segs, nseg, idx);
-            const int N = it.N, B = it.B, nt = it.nt;
-            if (DIR == 0 && lane < 16 && (g % kLoadWarps) == L) {
-                // the next item's bin columns into L2 while this one runs
-                const int nx = cta_item(r + 1, n_items);
-                if (nx >= 0) {
-                    const ItemGeo in = item_geo<DIR>(groups, segs, nseg, nx);
-                    const int t = lane >> 3, q = lane & 7;
-                    if (t < in.nt && q < in.nc) {
-                        const PairCase p = class_case(in.M, in.Mp, q, in.N);
-                        prefetch_l2(in.gr->X[in.t0 + t] + ((size_t)p.row * in.N + p.col) * in.N, (unsigned)in.N * 16u);
-                    }
-                }
-            }
-            // per-lane column scales of the columns this lane converts: task e = lane + 32 i
-            // is (octet o = e % 4, column pair cp = e / 4 = 2 (case) + transform), i < 2 * nt
+            const int N = it.N;
+            const int t = lane / 9, j = lane - 9 * (lane / 9);
+            const bool tl = t < it.nt;
+            const double2* aux = aux_of(it.gr, it.t0 + (tl ? t : 0));
+            PairCase p = class_case(it.M, it.Mp, (j < it.nc && j < 8) ? j : 0, N);
+            const long long ib = DIR == 1 ? inv_chunk_prefix(it.B, it.M, it.Mp) : 0;
+            bool stop = false;
             for (int c = 0; c < it.nchunks; ++c, ++g) {
-                if ((g % kLoadWarps) != L) continue;
-                const int s = g % kStages, u = g / kStages;
-                unsigned char* Bm = smem + s * kStageBytes + kABytes;
-                constexpr int kTasks = 8 * kNT * 4;   // column pairs x octets
-                double raw[kTasks / 32][8][2];
-                double2 mxv[kTasks / 32];   // the column's largest |re|, |im| (operand-scale table)
-                int tq[kTasks / 32], to[kTasks / 32];
-                // loads first (they fly while the stage is still being read by the MMAs): the data,
-                // the columns' scale-table entries, and (inverse) the row scale of degree
-                // M + 32c + lane, handed to the lanes that need it by shuffles below
-                double irs_lane = 0.0;
-                if (DIR == 1 && c * kKC + lane < it.R) irs_lane = __ldg(&row_table(it.gr, it.t0)[it.M + c * kKC + lane].y);
-#pragma unroll
-                for (int i = 0; i < kTasks / 32; ++i) {
-                    const int e = lane + 32 * i;
-                    const int o = e & 3, cpair = e >> 2;   // cpair = 8 t + q
-                    const int t = cpair >> 3, q = cpair & 7;
-                    tq[i] = cpair;
-                    to[i] = o;
-                    const bool live = t < nt && q < it.nc;
-                    {
-                        const double2* aux = it.gr->X[it.t0 + (live ? t : 0)] + (size_t)N * N * N;
-                        const PairCase p = class_case(it.M, it.Mp, live ? q : 0, N);
-                        mxv[i] = live ? (DIR == 0 ? __ldg(aux + (size_t)p.row * N + p.col) : __ldg(aux + (size_t)it.cls * 8 + q))
-                                      : make_double2(0.0, 0.0);
-                    }
+                const int slot = g % kRaw, u = g / kRaw;
+                if (!tc::mbar_wait_bounded(&bars[kBarRawEmpty + slot], (uint32_t)((u & 1) ^ 1), kWaitNs, s_abort)) {
+                    stop = true;
+                    break;
+                }
+                const int len = min(kKC, N - kKC * c);   // forward: beta samples of this chunk
+                const uint32_t per_t = DIR == 0 ? (uint32_t)(kRawHdr + it.nc * len * 16) : (uint32_t)(kRawHdr + 8 * kKC * 16);
+                if (lane == 0) tc::mbar_arrive_expect_tx(&bars[kBarRawFull + slot], per_t * (uint32_t)it.nt);
+                __syncwarp();
+                unsigned char* dst = smem + kOffRaw + slot * kRawBytes + t * kRawT;
+                if (tl && j == 8) {
+                    tc::bulk_g2s(dst, aux + (size_t)2 * 8 * it.cls, kRawHdr, &bars[kBarRawFull + slot]);
+                } else if (tl && j < 8) {
                     if (DIR == 0) {
-                        const PairCase p = class_case(it.M, it.Mp, live ? q : 0, N);
-                        const double2* col = it.gr->X[it.t0 + (live ? t : 0)] + ((size_t)p.row * N + p.col) * N;
-#pragma unroll
-                        for (int j = 0; j < 8; ++j) {
-                            const int k = c * kKC + 8 * o + j;
-                            double2 v = make_double2(0.0, 0.0);
-                            if (live && k < N) v = __ldg(col + (p.rev ? N - 1 - k : k));
-                            raw[i][j][0] = v.x;
-                            raw[i][j][1] = v.y;
+                        if (j < it.nc) {
+                            const int k0 = p.rev ? N - kKC * c - len : kKC * c;
+                            tc::bulk_g2s(dst + kRawHdr + j * kRawPitch,
+                                         it.gr->X[it.t0 + t] + ((size_t)p.row * N + p.col) * N + k0, (uint32_t)len * 16u,
+                                         &bars[kBarRawFull + slot]);
                         }
                     } else {
-                        const PairCase p = class_case(it.M, it.Mp, live ? q : 0, N);
-                        const double2* cf = it.gr->coeffs[it.t0 + (live ? t : 0)];
-#pragma unroll
-                        for (int j = 0; j < 8; ++j) {
-                            const int l = it.M + c * kKC + 8 * o + j;
-                            double2 v = make_double2(0.0, 0.0);
-                            if (live && l < B) v = __ldg(cf + coef_index(l, p.m1, p.m2));
-                            raw[i][j][0] = v.x;
-                            raw[i][j][1] = v.y;
-                        }
+                        tc::bulk_g2s(dst + kRawHdr + j * kRawPitch, aux + aux_inv(it.B) + (size_t)(ib + c) * 256 + j * kKC,
+                                     kKC * 16u, &bars[kBarRawFull + slot]);
                     }
                 }
-                if (!tc::mbar_wait_bounded(&bars[kBarEmpty + s], (uint32_t)((u & 1) ^ 1), kWaitNs, s_abort)) break;
-#pragma unroll
-                for (int i = 0; i < kTasks / 32; ++i) {
-                    const int cpair = tq[i], o = to[i];
-                    const int t = cpair >> 3, q = cpair & 7;
-                    double irs8[8];
-                    if (DIR == 1) {
-#pragma unroll
-                        for (int j = 0; j < 8; ++j) irs8[j] = __shfl_sync(0xffffffffu, irs_lane, 8 * o + j);
-                    }
-                    if (t >= nt || q >= it.nc) continue;   // columns never stored: left as they are
-                    const double2 mx = mxv[i];
-                    const double sgn_norm = DIR == 0 ? 1.0 : (double)(B * 2 * B) / kPi;   // src/fn_idsoft.cpp:109
-                    PairCase p = class_case(it.M, it.Mp, q, N);
-                    double cs_re, cs_im, ics_unused;
-                    column_scale(mx.x, cs_re, ics_unused);
-                    column_scale(mx.y, cs_im, ics_unused);
+                __syncwarp();
+            }
+            if (stop || *s_abort) break;
+        }
+        // the copies of the last armed phase of each slot have landed before the CTA can end
+        for (int k = 1; k <= kRaw && g - k >= 0; ++k) {
+            const int gg = g - k;
+            const uint64_t t0 = tc::globaltimer_ns();
+            while (!tc::mbar_try_wait(&bars[kBarRawFull + gg % kRaw], (uint32_t)((gg / kRaw) & 1)))
+                if (tc::globaltimer_ns() - t0 > kWaitNs) break;
+        }
+    } else if (warp >= kConvWarp0 && warp < kConvWarp0 + kConvWarps) {
+        // ------------------------------------------------------------------ digitise the data operand
+        // lane = 8 o + q: case q, beta / degree octet o of the chunk (a quarter warp reads the
+        // eight cases of one octet: distinct bank groups)
+        const int L = warp - kConvWarp0;
+        const int q = lane & 7, o = lane >> 3;
+        int g = 0;
+        for (int r = 0;; ++r) {
+            const int idx = cta_item(r, n_items);
+            if (idx < 0 || *s_abort) break;
+            const ItemGeo it = item_geo<DIR>(groups, segs, nseg, idx);
+            const int N = it.N;
+            const PairCase p = class_case(it.M, it.Mp, q < it.nc ? q : 0, N);
+            bool stop = false;
+            for (int c = 0; c < it.nchunks; ++c, ++g) {
+                if ((g % kConvWarps) != L) continue;
+                const int slot = g % kRaw, u = g / kRaw;
+                const int s = g % kStages, us = g / kStages;
+                if (!tc::mbar_wait_bounded(&bars[kBarRawFull + slot], (uint32_t)(u & 1), kWaitNs, s_abort) ||
+                    !tc::mbar_wait_bounded(&bars[kBarEmpty + s], (uint32_t)((us & 1) ^ 1), kWaitNs, s_abort)) {
+                    stop = true;
+                    break;
+                }
+                const unsigned char* raw = smem + kOffRaw + slot * kRawBytes;
+                unsigned char* Bm = smem + s * kStageBytes + kABytes;
+                const int len = min(kKC, N - kKC * c);
+                for (int t = 0; t < it.nt; ++t) {
+                    if (q >= it.nc) continue;   // rows of absent cases are never read back
+                    const double2 cs = *reinterpret_cast<const double2*>(raw + t * kRawT + 32 * q);
+                    const double2* col = reinterpret_cast<const double2*>(raw + t * kRawT + kRawHdr + q * kRawPitch);
                     double zr[8], zi[8];
-                    if (DIR == 0) {
 #pragma unroll
-                        for (int j = 0; j < 8; ++j) {
-                            zr[j] = fma(raw[i][j][0], cs_re, kMagic);
-                            zi[j] = fma(raw[i][j][1], cs_im, kMagic);
+                    for (int i = 0; i < 8; ++i) {
+                        const int kk = 8 * o + i;   // position in the chunk
+                        double2 v = make_double2(0.0, 0.0);
+                        if (DIR == 0) {
+                            if (kk < len) v = col[p.rev ? len - 1 - kk : kk];
+                        } else {
+                            v = col[kk];   // zero past the class's last degree
                         }
-                    } else {
-                        // G = norm * sign(l) * f / (row scale), zero past the last degree
-#pragma unroll
-                        for (int j = 0; j < 8; ++j) {
-                            const int l = it.M + c * kKC + 8 * o + j;
-                            double f = 0.0;
-                            if (l < B) f = sgn_norm * case_sign(p, l, it.M) * irs8[j];
-                            zr[j] = fma(f * raw[i][j][0], cs_re, kMagic);
-                            zi[j] = fma(f * raw[i][j][1], cs_im, kMagic);
-                        }
+                        zr[i] = fma(v.x, cs.x, kMagic);
+                        zi[i] = fma(v.y, cs.y, kMagic);
                     }
-                    const int n = 16 * t + 2 * q;   // re column; im is n + 1
-                    const int plane_rows = 16 * nt;
-                    // rows n, n+1 of plane 0; plane p at rows + 16 nt p: (n/8)*256 + (k/16)*128 + (n%8)*16 + k%16
-                    unsigned char* unit = Bm + (n >> 3) * 256 + (o >> 1) * 128 + (n & 7) * 16 + (o & 1) * 8;
-                    const int pstride = plane_rows / 8 * 256;
-                    store_unit8(unit, pstride, zr);
-                    store_unit8(unit + 16, pstride, zi);
+                    const int n = 2 * q;   // re row; im is n + 1
+                    unsigned char* unit = Bm + t * kBT + (n >> 3) * 256 + (o >> 1) * 128 + (n & 7) * 16 + (o & 1) * 8;
+                    store_unit8(unit, kBPlane, zr);
+                    store_unit8(unit + 16, kBPlane, zi);
                 }
                 tc::fence_proxy_async();
                 __syncwarp();
-                if (lane == 0) tc::mbar_arrive(&bars[kBarFull + s]);
+                if (lane == 0) {
+                    tc::mbar_arrive(&bars[kBarFull + s]);
+                    tc::mbar_arrive(&bars[kBarRawEmpty + slot]);
+                }
             }
-            if (*s_abort) break;
+            if (stop || *s_abort) break;
         }
     } else if (warp >= kEpiWarp0 && warp < kEpiWarp0 + 4) {
         // ------------------------------------------------------------------ epilogue
+        // The next item's column scales (lane i < 16: transform i / 8, case i % 8) and, forward, the
+        // lane's row scale are loaded while the current item is read back; the current item's
+        // column scales go through the warp's shared-memory slot.
         const int q4 = warp & 3;   // tensor-memory lane quarter
+        const int row = 32 * q4 + lane;
+        double2* s_ics = reinterpret_cast<double2*>(smem + kOffEpi) + 16 * q4;
+        auto next_item = [&](int& r) -> int {
+            for (;; ++r) {
+                const int idx = cta_item(r, n_items);
+                if (idx < 0) return -1;
+                if (item_geo<DIR>(groups, segs, nseg, idx).nchunks > 0) return idx;
+            }
+        };
+        auto load_scales = [&](const ItemGeo& it, double2& ics, double& rowf) {
+            const int t = lane >> 3, q = lane & 7;
+            ics = make_double2(1.0, 1.0);
+            if (lane < 16 && t < it.nt && q < it.nc) ics = __ldg(aux_of(it.gr, it.t0 + t) + (size_t)2 * (8 * it.cls + q) + 1);
+            rowf = 0.0;
+            const int l = it.M + 128 * it.tile + row;
+            if (DIR == 0 && l < it.B) rowf = (kPi / (double)(it.B * 2 * it.B)) * __ldg(&aux_of(it.gr, it.t0)[aux_rows(it.B) + l].y);   // src/fn_dsoft.cpp:119
+        };
+        int r = 0;
+        int idx = next_item(r);
+        ItemGeo it{};
+        double2 ics_c = make_double2(1.0, 1.0);
+        double rowf_c = 0.0;
+        if (idx >= 0) {
+            it = item_geo<DIR>(groups, segs, nseg, idx);
+            load_scales(it, ics_c, rowf_c);
+        }
         int n = 0;
-        for (int r = 0;; ++r) {
-            const int idx = cta_item(r, n_items);
-            if (idx < 0) break;
-            const ItemGeo it = item_geo<DIR>(groups, segs, nseg, idx);
-            if (it.nchunks == 0) continue;
+        while (idx >= 0) {
+            ++r;
+            const int nidx = next_item(r);
+            ItemGeo nit{};
+            double2 ics_n = make_double2(1.0, 1.0);
+            double rowf_n = 0.0;
+            if (nidx >= 0) {
+                nit = item_geo<DIR>(groups, segs, nseg, nidx);
+                load_scales(nit, ics_n, rowf_n);
+            }
             const int a = n & 1, ua = n >> 1;
             ++n;
             if (!tc::mbar_wait_bounded(&bars[kBarAccFull + a], (uint32_t)(ua & 1), kWaitNs, s_abort)) break;
             tc::fence_after_sync();
+            __syncwarp();
+            if (lane < 16) s_ics[lane] = ics_c;
+            __syncwarp();
             const int N = it.N, B = it.B;
-            const int row = 32 * q4 + lane;
             const uint32_t taddr = tmem + ((uint32_t)(32 * q4) << 16) + (uint32_t)(a * kAccStride);
-            const int cols = 16 * it.nt;
             // forward: degree l of this lane; inverse: beta k
             const int l = it.M + 128 * it.tile + row;
             const int k = 128 * it.tile + row;
             const bool live = DIR == 0 ? (l < B) : (k < N);
-            double rowf = 0.0;
-            if (DIR == 0 && live) rowf = (kPi / (double)(B * 2 * B)) * __ldg(&row_table(it.gr, it.t0)[l].y);   // src/fn_dsoft.cpp:119
             for (int t = 0; t < it.nt; ++t) {
-                // the eight columns' scale-table entries, in flight while the accumulators are read
-                const double2* aux = it.gr->X[it.t0 + t] + (size_t)N * N * N;
-                double2 mxq[8];
-#pragma unroll
-                for (int q = 0; q < 8; ++q) {
-                    mxq[q] = make_double2(0.0, 0.0);
-                    if (q < it.nc) {
-                        const PairCase p = class_case(it.M, it.Mp, q, N);
-                        mxq[q] = DIR == 0 ? __ldg(aux + (size_t)p.row * N + p.col) : __ldg(aux + (size_t)it.cls * 8 + q);
-                    }
-                }
                 int32_t acc[kPlanes][16];
 #pragma unroll
-                for (int e = 0; e < kPlanes; ++e) tc::tmem_ld16(taddr + (uint32_t)(cols * e + 16 * t), acc[e]);
+                for (int e = 0; e < kPlanes; ++e) tc::tmem_ld16(taddr + (uint32_t)(kAccT * t + 16 * e), acc[e]);
                 tc::tmem_wait_ld();
                 double v[16];
 #pragma unroll
                 for (int j = 0; j < 16; ++j) {
-                    double h = (double)acc[5][j];
-                    h = fma(h, 0x1p-8, (double)acc[4][j]);
-                    h = fma(h, 0x1p-8, (double)acc[3][j]);
-                    h = fma(h, 0x1p-8, (double)acc[2][j]);
-                    h = fma(h, 0x1p-8, (double)acc[1][j]);
-                    v[j] = fma(h, 0x1p-8, (double)acc[0][j]) * 0x1p-14;
+                    // sum_e acc[e] 2^(-8e) = 2^-16 (hi + 2^-24 lo), hi and lo exact in 64 bits
+                    const long long hi = (long long)acc[0][j] * 65536 + (long long)acc[1][j] * 256 + acc[2][j];
+                    const long long lo = (long long)acc[3][j] * 65536 + (long long)acc[4][j] * 256 + acc[5][j];
+                    v[j] = fma((double)lo, 0x1p-24, (double)hi) * 0x1p-30;   // and the digits' 2^-14
                 }
                 if (!live) continue;
 #pragma unroll
                 for (int q = 0; q < 8; ++q) {
                     if (q >= it.nc) break;
                     const PairCase p = class_case(it.M, it.Mp, q, N);
-                    const double2 mx = mxq[q];
-                    double unused, ics_re, ics_im;
-                    column_scale(mx.x, unused, ics_re);
-                    column_scale(mx.y, unused, ics_im);
+                    const double2 ics = s_ics[8 * t + q];
                     if (DIR == 0) {
-                        const double f = rowf * case_sign(p, l, it.M);
+                        const double f = rowf_c * case_sign(p, l, it.M);
                         it.gr->coeffs[it.t0 + t][coef_index(l, p.m1, p.m2)] =
-                            make_double2(f * v[2 * q] * ics_re, f * v[2 * q + 1] * ics_im);
+                            make_double2(f * v[2 * q] * ics.x, f * v[2 * q + 1] * ics.y);
                     } else {
                         it.gr->X[it.t0 + t][((size_t)p.row * N + p.col) * N + (p.rev ? N - 1 - k : k)] =
-                            make_double2(v[2 * q] * ics_re, v[2 * q + 1] * ics_im);
+                            make_double2(v[2 * q] * ics.x, v[2 * q + 1] * ics.y);
                     }
                 }
             }
             tc::fence_before_sync();
             __syncwarp();
             if (lane == 0) tc::mbar_arrive(&bars[kBarAccEmpty + a]);
+            idx = nidx;
+            it = nit;
+            ics_c = ics_n;
+            rowf_c = rowf_n;
         }
     } else if (warp >= kGenWarp0) {
         // ------------------------------------------------------------------ generators (Wigner rows)
         // The recurrence coefficients and row scales of 32 steps at a time are loaded by the warp's
         // lanes in one coalesced load (a batch ahead, into registers) and published to the warp's
         // shared-memory slot; the steps read them from there, so no step waits on global memory.
+        // Rows past the class's last degree get zero coefficients and a zero row scale.
         const int w = warp - kGenWarp0;
         double* s_cf = reinterpret_cast<double*>(smem + kOffCoef) + w * 128;
         double2 pcf = make_double2(0.0, 0.0);
@@ -546,7 +631,8 @@ __global__ void __launch_bounds__(kThreads, 1)
             const DwtGroup* gr = it.gr;
             const long long rc0 = rc_offset(it.B, it.M, it.Mp);
             const double nf = gr->normf[it.cls];
-            const double2* rows = row_table(gr, it.t0);
+            const double2* rows = aux_of(gr, it.t0) + aux_rows(it.B);
+            bool stop = false;
             if (DIR == 0) {
                 // forward: this warp's chunks (beta columns 32c + lane), rows of the item's tile
                 const int r0 = 128 * it.tile, rn = min(R - r0, 128), end = r0 + rn;
@@ -561,16 +647,25 @@ __global__ void __launch_bounds__(kThreads, 1)
                         dcur = seed_value(nf * gr->w[k], gr->pw_sin[(size_t)(it.M - it.Mp) * N + k],
                                           gr->pw_cos[(size_t)(it.M + it.Mp) * N + k], sc);
                     }
+                    bool scaled = __any_sync(0xffffffffu, sc > 0);
                     fetch(gr, rc0, rows, M, R, 0);
                     int base = 0;
                     for (; base < r0; base += 32) {   // second row tile: run through the first 128 degrees
                         publish();
                         fetch(gr, rc0, rows, M, R, base + 32);
-#pragma unroll 8
-                        for (int j = 0; j < 32; ++j)
-                            rec_step(dcur, dprev, sc, cb, *reinterpret_cast<const double2*>(s_cf + 4 * j), s_cf[4 * j + 2]);
+#pragma unroll 1
+                        for (int h = 0; h < 2; ++h) {
+                            adv16(dcur, dprev, cb, s_cf, 16 * h);
+                            if (scaled) {
+                                rescale_check(dcur, dprev, sc);
+                                scaled = __any_sync(0xffffffffu, sc > 0);
+                            }
+                        }
                     }
-                    if (!tc::mbar_wait_bounded(&bars[kBarEmpty + s], (uint32_t)((u & 1) ^ 1), kWaitNs, s_abort)) break;
+                    if (!tc::mbar_wait_bounded(&bars[kBarEmpty + s], (uint32_t)((u & 1) ^ 1), kWaitNs, s_abort)) {
+                        stop = true;
+                        break;
+                    }
                     unsigned char* A = smem + s * kStageBytes + lane * 16;   // (k/8)*128 + (k%8)*16 = lane*16
                     for (; base < end; base += 32) {
                         publish();
@@ -580,15 +675,10 @@ __global__ void __launch_bounds__(kThreads, 1)
                             const int b16 = base + 16 * h;
                             if (b16 >= end) break;
                             double z[16];
-#pragma unroll
-                            for (int j = 0; j < 16; ++j) {
-                                const int q = 16 * h + j;
-                                if (b16 + j < R) {
-                                    z[j] = fma(sc ? 0.0 : dcur, s_cf[4 * q + 3], kMagic);
-                                    rec_step(dcur, dprev, sc, cb, *reinterpret_cast<const double2*>(s_cf + 4 * q), s_cf[4 * q + 2]);
-                                } else {
-                                    z[j] = kMagic;
-                                }
+                            gen16(z, dcur, dprev, sc, cb, s_cf, 16 * h);
+                            if (scaled) {
+                                rescale_check(dcur, dprev, sc);
+                                scaled = __any_sync(0xffffffffu, sc > 0);
                             }
                             if (k < N) store_unit16(A + ((b16 - r0) >> 4) * 512, kAPlane, z);
                         }
@@ -607,25 +697,24 @@ __global__ void __launch_bounds__(kThreads, 1)
                     cb = gr->cosb[k];
                     dcur = seed_value(nf, gr->pw_sin[(size_t)(it.M - it.Mp) * N + k], gr->pw_cos[(size_t)(it.M + it.Mp) * N + k], sc);
                 }
+                bool scaled = __any_sync(0xffffffffu, sc > 0);
                 fetch(gr, rc0, rows, M, R, 0);
                 for (int c = 0; c < it.nchunks; ++c, ++g) {
                     const int s = g % kStages, u = g / kStages;
                     publish();
                     fetch(gr, rc0, rows, M, R, (c + 1) * kKC);
-                    if (!tc::mbar_wait_bounded(&bars[kBarEmpty + s], (uint32_t)((u & 1) ^ 1), kWaitNs, s_abort)) break;
+                    if (!tc::mbar_wait_bounded(&bars[kBarEmpty + s], (uint32_t)((u & 1) ^ 1), kWaitNs, s_abort)) {
+                        stop = true;
+                        break;
+                    }
                     unsigned char* A = smem + s * kStageBytes + (m >> 3) * 256 + (m & 7) * 16;
 #pragma unroll 1
                     for (int h = 0; h < 2; ++h) {
                         double z[16];
-#pragma unroll
-                        for (int j = 0; j < 16; ++j) {
-                            const int q = 16 * h + j;
-                            if (c * kKC + q < R) {
-                                z[j] = fma(sc ? 0.0 : dcur, s_cf[4 * q + 3], kMagic);
-                                rec_step(dcur, dprev, sc, cb, *reinterpret_cast<const double2*>(s_cf + 4 * q), s_cf[4 * q + 2]);
-                            } else {
-                                z[j] = kMagic;
-                            }
+                        gen16(z, dcur, dprev, sc, cb, s_cf, 16 * h);
+                        if (scaled) {
+                            rescale_check(dcur, dprev, sc);
+                            scaled = __any_sync(0xffffffffu, sc > 0);
                         }
                         store_unit16(A + h * 128, kAPlane, z);
                     }
@@ -634,7 +723,7 @@ __global__ void __launch_bounds__(kThreads, 1)
                     if (lane == 0) tc::mbar_arrive(&bars[kBarFull + s]);
                 }
             }
-            if (*s_abort) break;
+            if (stop || *s_abort) break;
         }
     }
 
@@ -647,51 +736,93 @@ __global__ void __launch_bounds__(kThreads, 1)
     }
 }
 
-// Largest |re|, |im| over beta of every bin column of a spectrum, into the table past it
-// (forward operand scales). One warp per bin, gridDim.z = transforms.
-__global__ void split_binmax_kernel(double2* const* X, int N)
+// Forward column scales: for every (class, case) the largest |re|, |im| over beta of its bin
+// column, as {scale * 2^47} and {1 / scale} into the transform's scale table. One warp per
+// (class, case), gridDim.z = transforms.
+__global__ void split_fwd_scales_kernel(double2* const* X, int B)
 {
-    const long long bin = (long long)blockIdx.x * 8 + (threadIdx.x >> 5);
+    const int N = 2 * B;
+    const long long wid = (long long)blockIdx.x * 8 + (threadIdx.x >> 5);
     const int lane = threadIdx.x & 31;
-    if (bin >= (long long)N * N) return;
-    const double2* col = X[blockIdx.z] + bin * N;
+    if (wid >= (long long)num_classes(B) * 8) return;
+    const int cls = (int)(wid >> 3), q = (int)(wid & 7);
+    int M, Mp;
+    class_orders(cls, M, Mp);
     double mre = 0.0, mim = 0.0;
-    for (int k = lane; k < N; k += 32) {
-        const double2 v = __ldg(col + k);
-        mre = fmax(mre, fabs(v.x));
-        mim = fmax(mim, fabs(v.y));
+    if (q < class_case_count(M, Mp)) {
+        const PairCase p = class_case(M, Mp, q, N);
+        const double2* col = X[blockIdx.z] + ((size_t)p.row * N + p.col) * N;
+        for (int k = lane; k < N; k += 32) {
+            const double2 v = __ldg(col + k);
+            mre = fmax(mre, fabs(v.x));
+            mim = fmax(mim, fabs(v.y));
+        }
     }
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) {
         mre = fmax(mre, __shfl_xor_sync(0xffffffffu, mre, o));
         mim = fmax(mim, __shfl_xor_sync(0xffffffffu, mim, o));
     }
-    if (lane == 0) X[blockIdx.z][(size_t)N * N * N + bin] = make_double2(mre, mim);
+    if (lane == 0) {
+        double cr, ci, ir, ii;
+        column_scale(mre, cr, ir);
+        column_scale(mim, ci, ii);
+        double2* tab = X[blockIdx.z] + (size_t)N * N * N + (size_t)2 * wid;
+        tab[0] = make_double2(cr, ci);
+        tab[1] = make_double2(ir, ii);
+    }
 }
 
-// Largest |re|, |im| over the degrees of each (class, case) of the inverse operand
-// norm * coefficient / (row scale), into the table past the spectrum. One thread per (class, case).
-__global__ void split_coefmax_kernel(double2* const* X, const double2* const* coeffs, int B)
+// Inverse operand: for every (class, case) the column G[l] = (2B^2/pi) sign(l) f^l / (row scale of
+// l), l = M..B-1 (src/fn_idsoft.cpp:109), written class-major (chunk c of the class: 8 cases x 32
+// degrees, zero past B - 1 and for absent cases), and its column scales into the scale table.
+// One warp per (class, case), gridDim.z = transforms; the row table must be written first.
+__global__ void split_inv_prepare_kernel(double2* const* X, const double2* const* coeffs, int B)
 {
     const int N = 2 * B;
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= num_classes(B) * 8) return;
-    const int cls = i >> 3, q = i & 7;
+    const long long wid = (long long)blockIdx.x * 8 + (threadIdx.x >> 5);
+    const int lane = threadIdx.x & 31;
+    if (wid >= (long long)num_classes(B) * 8) return;
+    const int cls = (int)(wid >> 3), q = (int)(wid & 7);
     int M, Mp;
     class_orders(cls, M, Mp);
+    const int nch = (B - M + kKC - 1) / kKC;
+    double2* aux = X[blockIdx.z] + (size_t)N * N * N;
+    const double2* rows = aux + aux_rows(B);
+    const bool live = q < class_case_count(M, Mp);
+    const PairCase p = class_case(M, Mp, live ? q : 0, N);
+    const double2* cf = coeffs[blockIdx.z];
+    const double norm = (double)(B * 2 * B) / kPi;
+    double2 v[8];
     double mre = 0.0, mim = 0.0;
-    if (q < class_case_count(M, Mp)) {
-        const PairCase p = class_case(M, Mp, q, N);
-        const double2* cf = coeffs[blockIdx.z];
-        const double norm = (double)(B * 2 * B) / kPi;
-        for (int l = M; l < B; ++l) {
-            const double f = norm * (sqrt((double)l + 0.5) / 0.49);
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+        v[i] = make_double2(0.0, 0.0);
+        const int l = M + kKC * i + lane;
+        if (i < nch && live && l < B) {
+            const double f = norm * case_sign(p, l, M) * __ldg(&rows[l].y);
             const double2 x = __ldg(cf + coef_index(l, p.m1, p.m2));
-            mre = fmax(mre, fabs(f * x.x));
-            mim = fmax(mim, fabs(f * x.y));
+            v[i] = make_double2(f * x.x, f * x.y);
+            mre = fmax(mre, fabs(v[i].x));
+            mim = fmax(mim, fabs(v[i].y));
         }
     }
-    X[blockIdx.z][(size_t)N * N * N + i] = make_double2(mre, mim);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        mre = fmax(mre, __shfl_xor_sync(0xffffffffu, mre, o));
+        mim = fmax(mim, __shfl_xor_sync(0xffffffffu, mim, o));
+    }
+    double2* out = aux + aux_inv(B) + (size_t)inv_chunk_prefix(B, M, Mp) * 256 + q * kKC + lane;
+#pragma unroll
+    for (int i = 0; i < 8; ++i)
+        if (i < nch) out[(size_t)i * 256] = v[i];
+    if (lane == 0) {
+        double cr, ci, ir, ii;
+        column_scale(mre, cr, ir);
+        column_scale(mim, ci, ii);
+        aux[2 * wid] = make_double2(cr, ci);
+        aux[2 * wid + 1] = make_double2(ir, ii);
+    }
 }
 
 // Row scales of the generated operand, {0.49 / bound * 2^47, bound / 0.49} per degree l, bound =
@@ -713,8 +844,7 @@ __global__ void split_rows_kernel(double2* const* X, const double* w, int B, int
         wmax = red[0];
         for (int i = 1; i < (int)(blockDim.x >> 5); ++i) wmax = fmax(wmax, red[i]);
     }
-    const size_t a0 = (size_t)N * N > (size_t)8 * num_classes(B) ? (size_t)N * N : (size_t)8 * num_classes(B);
-    double2* rows = X[blockIdx.z] + (size_t)N * N * N + a0;
+    double2* rows = X[blockIdx.z] + (size_t)N * N * N + aux_rows(B);
     for (int l = threadIdx.x; l < B; l += blockDim.x) {
         const double bound = wmax * sqrt((double)l + 0.5);
         const double rs = 0.49 / bound;
@@ -728,24 +858,20 @@ bool dwt_split_supported(int B) { return B >= 1 && B <= 256; }
 
 size_t dwt_split_aux_elems(int B)
 {
-    const size_t n2 = (size_t)4 * B * B, c8 = (size_t)8 * num_classes(B);
-    return (n2 > c8 ? n2 : c8) + (size_t)B;
+    return aux_inv(B) + (size_t)256 * (size_t)inv_chunk_prefix(B, B, 0);
 }
 
 cudaError_t dwt_split_scales(int direction, int B, int T, double2* const* d_ws, const double2* const* d_coeffs,
                              const double* w, cudaStream_t s)
 {
-    const int N = 2 * B;
-    if (direction == 0) {
-        dim3 grid((unsigned)(((long long)N * N + 7) / 8), 1, (unsigned)T);
-        split_binmax_kernel<<<grid, 256, 0, s>>>(d_ws, N);
-    } else {
-        dim3 grid((unsigned)((num_classes(B) * 8 + 255) / 256), 1, (unsigned)T);
-        split_coefmax_kernel<<<grid, 256, 0, s>>>(d_ws, d_coeffs, B);
-    }
+    split_rows_kernel<<<dim3(1, 1, (unsigned)T), 256, 0, s>>>(d_ws, w, B, direction == 0 ? 1 : 0);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
-    split_rows_kernel<<<dim3(1, 1, (unsigned)T), 256, 0, s>>>(d_ws, w, B, direction == 0 ? 1 : 0);
+    dim3 grid((unsigned)((num_classes(B) * 8 + 7) / 8), 1, (unsigned)T);
+    if (direction == 0)
+        split_fwd_scales_kernel<<<grid, 256, 0, s>>>(d_ws, B);
+    else
+        split_inv_prepare_kernel<<<grid, 256, 0, s>>>(d_ws, d_coeffs, B);
     return cudaGetLastError();
 }
 

@@ -1,6 +1,7 @@
 // Thin wrappers over the sm_100a instructions used by the split-precision DWT: tcgen05.* with
-// operands in shared memory and the accumulator in tensor memory, the mbarrier operations that
-// order them, and the async-proxy fences. Inline PTX, one instruction per function.
+// operands in shared memory and the accumulator in tensor memory, untiled bulk copies from global
+// memory into shared memory, the mbarrier operations that order them, and the async-proxy
+// fences. Inline PTX, one instruction per function.
 //
 // Shared-memory operand layouts (no swizzle, 8-bit elements): the tensor core reads "core
 // matrices" of 8 rows x 16 bytes, each 128 contiguous bytes.
@@ -106,6 +107,25 @@ __device__ __forceinline__ void mbar_fence_init() { asm volatile("fence.mbarrier
 __device__ __forceinline__ void mbar_arrive(uint64_t* mbar)
 {
     asm volatile("{\n\t.reg .b64 st;\n\tmbarrier.arrive.shared::cta.b64 st, [%0];\n\t}" ::"r"(smem_u32(mbar)) : "memory");
+}
+
+// Arrives once and adds `bytes` to the transaction count the current phase waits for.
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t* mbar, uint32_t bytes)
+{
+    asm volatile("{\n\t.reg .b64 st;\n\tmbarrier.arrive.expect_tx.shared::cta.b64 st, [%0], %1;\n\t}" ::"r"(smem_u32(mbar)),
+                 "r"(bytes)
+                 : "memory");
+}
+
+// ---- bulk copy global -> shared (untiled, no multicast), completion on an mbarrier ------------
+// Both addresses 16-byte aligned, `bytes` a multiple of 16; the destination is this CTA's own
+// shared memory.
+__device__ __forceinline__ void bulk_g2s(void* dst_smem, const void* src_gmem, uint32_t bytes, uint64_t* mbar)
+{
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(smem_u32(dst_smem)),
+        "l"(src_gmem), "r"(bytes), "r"(smem_u32(mbar))
+        : "memory");
 }
 
 __device__ __forceinline__ bool mbar_try_wait(uint64_t* mbar, uint32_t parity)
