@@ -46,7 +46,7 @@ __host__ __device__ __forceinline__ size_t coef_index(int l, int m1, int m2)
 // (B - M degrees), i.e. longest-first order for the schedulers.
 __host__ __device__ __forceinline__ void class_orders(int i, int& M, int& Mp)
 {
-    int m = (int)((sqrt(8.0 * i + 1.0) - 1.0) * 0.5);
+    int m = (int)((sqrtf(8.0f * (float)i + 1.0f) - 1.0f) * 0.5f);   // corrected below: exact for any i
     while (m * (m + 1) / 2 > i) --m;
     while ((m + 1) * (m + 2) / 2 <= i) ++m;
     M = m;

@@ -52,9 +52,9 @@
 // Operand layouts in shared memory (no swizzle; see tc_sm100.cuh), per stage and plane:
 //   A forward (MN-major, rows = degrees):  (r/16)*512 + (k/8)*128 + (k%8)*16 + (r%16)
 //   A inverse (K-major, rows = beta):      (m/8)*256 + (j/16)*128 + (m%8)*16 + (j%16)
-//   B both    (K-major): transform t at t*3072, plane p at +p*512, row n = 2 case + (re, im):
-//             (n/8)*256 + (k/16)*128 + (n%8)*16 + (k%16)  -- a transform's planes are contiguous,
-//             so planes 0..5-s of one transform are one B operand of N = 16 (6 - s) rows.
+//   B both    (K-major, rows = columns):   (n/8)*256 + (k/16)*128 + (n%8)*16 + (k%16), row n =
+//             16 nt p + 16 t + 2 case + (re, im) for plane p of transform t (planes concatenated
+//             along N, so planes 0..5-s of every transform are one B operand of N = 16 nt (6 - s)).
 // The generator inner loops carry no data-dependent branch: rows past the class's last degree
 // get zero recurrence coefficients and a zero row scale (digits 0), and a column still scaled by
 // 2^600 (tiny seed, see dwt.cu) is checked for its rescale once per 16 degrees.
@@ -96,7 +96,6 @@ constexpr int kStages = 6;             // operand ring
 constexpr int kRaw = 4;                // raw-data ring
 constexpr int kAccSets = 2;
 constexpr int kAccStride = 256;        // tensor-memory columns between the two accumulator sets
-constexpr int kAccT = 16 * kPlanes;    // accumulator columns per transform: 6 planes x 16
 constexpr uint32_t kTmemCols = 512;
 constexpr int kThreads = 384;
 constexpr int kCopyWarp = 1;
@@ -107,9 +106,8 @@ constexpr uint64_t kWaitNs = 2000000000ull;   // 2 s
 
 constexpr int kAPlane = 4096;                       // 128 rows x 32 bytes of K
 constexpr int kABytes = kPlanes * kAPlane;          // 24 KB
-constexpr int kBPlane = 512;                        // 16 rows x 32 bytes of K
-constexpr int kBT = kPlanes * kBPlane;              // one transform's planes: 3 KB
-constexpr int kBBytes = kNT * kBT;                  // 6 KB
+constexpr int kBRows = 16 * kNT * kPlanes;          // 192
+constexpr int kBBytes = kBRows / 8 * 256;           // 6 KB
 constexpr int kStageBytes = kABytes + kBBytes;
 // raw slot, per transform: 8 scale entries {cs47 re, im}, {1/scale re, im} (256 B), then the 8
 // cases' 32 double2 each at a 528-byte pitch (a quarter warp reading one value of each case hits
@@ -121,7 +119,9 @@ constexpr int kRawBytes = kNT * kRawT;
 constexpr int kOffRaw = kStages * kStageBytes;
 constexpr int kOffCoef = kOffRaw + kRaw * kRawBytes;   // generators: 32 steps x {c1, f1 f2, f1, row scale} per warp
 constexpr int kOffEpi = kOffCoef + kGenWarps * 32 * 4 * 8;   // epilogue: 16 x {1/scale re, im} per warp
-constexpr int kOffBar = kOffEpi + 4 * 16 * 16;
+constexpr int kSegCache = 256;                      // segment starts kept in shared memory
+constexpr int kOffSeg = kOffEpi + 4 * 16 * 16;     // first item of each segment (the first kSegCache)
+constexpr int kOffBar = kOffSeg + kSegCache * 4;
 // mbarriers: full[kStages], empty[kStages], accfull[2], accempty[2], rawfull[kRaw], rawempty[kRaw],
 // drain, never (test knob)
 constexpr int kBarFull = 0, kBarEmpty = kStages, kBarAccFull = 2 * kStages, kBarAccEmpty = 2 * kStages + kAccSets,
@@ -131,8 +131,9 @@ constexpr int kOffMisc = kOffBar + kNumBars * 8;    // tensor-memory address, ab
 constexpr int kSmemBytes = kOffMisc + 16;
 static_assert(kStageBytes % 1024 == 0, "stages stay 1 KB aligned");
 static_assert(kRawT % 16 == 0 && kRawPitch % 16 == 0 && kOffRaw % 16 == 0, "bulk-copy destinations 16-byte aligned");
+constexpr int kInvChunk = kRawT / 16;               // double2 per inverse chunk block (280)
 static_assert(kSmemBytes <= 227 * 1024, "shared memory");
-static_assert(kNT * kAccT <= kAccStride, "an accumulator set fits its column range");
+static_assert(16 * kNT * kPlanes <= kAccStride, "an accumulator set fits its column range");
 
 constexpr double kTwo47 = 140737488355328.0;        // 2^47
 // 2^52 + sum_{i<6} 128 * 256^i: adding it to x * 2^47 (|x| < 0.5) leaves round(x * 2^47) + C in
@@ -140,14 +141,16 @@ constexpr double kTwo47 = 140737488355328.0;        // 2^47
 constexpr double kMagic = 4503599627370496.0 + 141289400074368.0;
 
 // One bandwidth group of a launch: items first .. first+count-1, `pairs` transform pairs (T
-// transforms) and `tiles` tiles per class.
+// transforms) and `tiles` tiles per class, bandwidth B, N = 2B.
 struct SplitSeg {
-    int group, first, count, pairs, tiles, T, pad0, pad1;
+    int group, first, count, pairs, tiles, T, B, N;
 };
 
 // Operand area past each transform's spectrum (double2 offsets from X + N^3): the column scale
 // table (two double2 per (class, case)), the row table (one per degree), the inverse operand in
-// class-major order (256 double2 per 32-degree chunk: 8 cases x 32 degrees).
+// class-major order, one block per 32-degree chunk laid out as a raw slot: the class's 8 scale
+// entries, then 8 cases x 32 degrees at the slot's pitch (kInvChunk double2), so that a chunk of
+// one transform is a single bulk copy.
 __host__ __device__ __forceinline__ size_t aux_rows(int B) { return (size_t)16 * num_classes(B); }
 __host__ __device__ __forceinline__ size_t aux_inv(int B) { return aux_rows(B) + (size_t)B; }
 
@@ -213,15 +216,23 @@ struct ItemGeo {
     int B, N, M, Mp, R, nc, t0, nt, tile, cls, nchunks;
 };
 
-// Geometry of item i: its segment by a scan over the launch's few segments, then class,
+__device__ __forceinline__ int seg_first(const SplitSeg* __restrict__ segs, const int* s_first, int j)
+{
+    return j < kSegCache ? s_first[j] : segs[j].first;
+}
+
+// Geometry of item i: its segment by a forward scan from the caller's hint (a role visits items
+// in increasing order, so the scan is short; the segment starts are in shared memory), then class,
 // transform pair and tile. A forward row tile past the class's last degree has no chunks (every
 // role skips it alike).
 template <int DIR>
 __device__ __forceinline__ ItemGeo item_geo(const DwtGroup* __restrict__ groups, const SplitSeg* __restrict__ segs,
-                                            int nseg, int i)
+                                            const int* s_first, int nseg, int i, int& hint)
 {
-    int sidx = 0;
-    while (sidx + 1 < nseg && i >= segs[sidx + 1].first) ++sidx;
+    int sidx = hint;
+    if (i < seg_first(segs, s_first, sidx)) sidx = 0;
+    while (sidx + 1 < nseg && i >= seg_first(segs, s_first, sidx + 1)) ++sidx;
+    hint = sidx;
     const SplitSeg sg = segs[sidx];
     const int j = i - sg.first;
     const int per_cls = sg.pairs * sg.tiles;
@@ -229,8 +240,8 @@ __device__ __forceinline__ ItemGeo item_geo(const DwtGroup* __restrict__ groups,
     const int pair = rem / sg.tiles;
     ItemGeo g;
     g.gr = groups + sg.group;
-    g.B = g.gr->B;
-    g.N = g.gr->N;
+    g.B = sg.B;
+    g.N = sg.N;
     class_orders(cls, g.M, g.Mp);
     g.R = g.B - g.M;
     g.nc = class_case_count(g.M, g.Mp);
@@ -312,6 +323,9 @@ __global__ void __launch_bounds__(kThreads, 1)
     uint32_t* s_taddr = reinterpret_cast<uint32_t*>(smem + kOffMisc);
     volatile int* s_abort = reinterpret_cast<volatile int*>(smem + kOffMisc + 4);
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    int* s_first = reinterpret_cast<int*>(smem + kOffSeg);
+    for (int j = tid; j < min(nseg, kSegCache); j += kThreads) s_first[j] = segs[j].first;
+    int hint = 0;   // this warp's segment cursor (items are visited in increasing order)
 
     if (warp == 0) {
         tc::tmem_alloc(s_taddr, kTmemCols);
@@ -349,7 +363,7 @@ __global__ void __launch_bounds__(kThreads, 1)
         for (int r = 0; ok; ++r) {
             const int idx = cta_item(r, n_items);
             if (idx < 0) break;
-            const ItemGeo it = item_geo<DIR>(groups, segs, nseg, idx);
+            const ItemGeo it = item_geo<DIR>(groups, segs, s_first, nseg, idx, hint);
             if (it.nchunks == 0) continue;
             const int a = n & 1, ua = n >> 1;
             ++n;
@@ -368,13 +382,13 @@ __global__ void __launch_bounds__(kThreads, 1)
                 tc::fence_after_sync();
                 if (lane == 0) {
                     const uint32_t a0 = smem_base + s * kStageBytes, b0 = a0 + kABytes;
+                    const uint64_t bd = tc::sdesc(b0, 128, 256);
+                    const int cols = 16 * it.nt;
 #pragma unroll
                     for (int p = 0; p < kPlanes; ++p) {
                         const uint64_t ad = DIR == 0 ? tc::sdesc(a0 + p * kAPlane, 128, 512) : tc::sdesc(a0 + p * kAPlane, 128, 256);
-                        const uint32_t id = tc::idesc_s8(128, 16 * (kPlanes - p), DIR == 0, false);
-                        for (int t = 0; t < it.nt; ++t)
-                            tc::mma_s8(dbase + (uint32_t)(kAccT * t + 16 * p), ad, tc::sdesc(b0 + t * kBT, 128, 256), id,
-                                       !(c == 0 && p == 0));
+                        tc::mma_s8(dbase + (uint32_t)(cols * p), ad, bd, tc::idesc_s8(128, cols * (kPlanes - p), DIR == 0, false),
+                                   !(c == 0 && p == 0));
                     }
                     tc::mma_commit(&bars[kBarEmpty + s]);
                 }
@@ -400,7 +414,7 @@ __global__ void __launch_bounds__(kThreads, 1)
         for (int r = 0;; ++r) {
             const int idx = cta_item(r, n_items);
             if (idx < 0 || *s_abort) break;
-            const ItemGeo it = item_geo<DIR>(groups, segs, nseg, idx);
+            const ItemGeo it = item_geo<DIR>(groups, segs, s_first, nseg, idx, hint);
             const int N = it.N;
             const int t = lane / 9, j = lane - 9 * (lane / 9);
             const bool tl = t < it.nt;
@@ -415,23 +429,24 @@ __global__ void __launch_bounds__(kThreads, 1)
                     break;
                 }
                 const int len = min(kKC, N - kKC * c);   // forward: beta samples of this chunk
-                const uint32_t per_t = DIR == 0 ? (uint32_t)(kRawHdr + it.nc * len * 16) : (uint32_t)(kRawHdr + 8 * kKC * 16);
+                const uint32_t per_t = DIR == 0 ? (uint32_t)(kRawHdr + it.nc * len * 16) : (uint32_t)kRawT;
                 if (lane == 0) tc::mbar_arrive_expect_tx(&bars[kBarRawFull + slot], per_t * (uint32_t)it.nt);
                 __syncwarp();
                 unsigned char* dst = smem + kOffRaw + slot * kRawBytes + t * kRawT;
-                if (tl && j == 8) {
+                if (DIR == 1) {
+                    // the chunk block of transform t (lane t < nt): header and data in one copy
+                    if (lane < it.nt)
+                        tc::bulk_g2s(smem + kOffRaw + slot * kRawBytes + lane * kRawT,
+                                     aux_of(it.gr, it.t0 + lane) + aux_inv(it.B) + (size_t)(ib + c) * kInvChunk, (uint32_t)kRawT,
+                                     &bars[kBarRawFull + slot]);
+                } else if (tl && j == 8) {
                     tc::bulk_g2s(dst, aux + (size_t)2 * 8 * it.cls, kRawHdr, &bars[kBarRawFull + slot]);
                 } else if (tl && j < 8) {
-                    if (DIR == 0) {
-                        if (j < it.nc) {
-                            const int k0 = p.rev ? N - kKC * c - len : kKC * c;
-                            tc::bulk_g2s(dst + kRawHdr + j * kRawPitch,
-                                         it.gr->X[it.t0 + t] + ((size_t)p.row * N + p.col) * N + k0, (uint32_t)len * 16u,
-                                         &bars[kBarRawFull + slot]);
-                        }
-                    } else {
-                        tc::bulk_g2s(dst + kRawHdr + j * kRawPitch, aux + aux_inv(it.B) + (size_t)(ib + c) * 256 + j * kKC,
-                                     kKC * 16u, &bars[kBarRawFull + slot]);
+                    if (j < it.nc) {
+                        const int k0 = p.rev ? N - kKC * c - len : kKC * c;
+                        tc::bulk_g2s(dst + kRawHdr + j * kRawPitch,
+                                     it.gr->X[it.t0 + t] + ((size_t)p.row * N + p.col) * N + k0, (uint32_t)len * 16u,
+                                     &bars[kBarRawFull + slot]);
                     }
                 }
                 __syncwarp();
@@ -455,7 +470,7 @@ __global__ void __launch_bounds__(kThreads, 1)
         for (int r = 0;; ++r) {
             const int idx = cta_item(r, n_items);
             if (idx < 0 || *s_abort) break;
-            const ItemGeo it = item_geo<DIR>(groups, segs, nseg, idx);
+            const ItemGeo it = item_geo<DIR>(groups, segs, s_first, nseg, idx, hint);
             const int N = it.N;
             const PairCase p = class_case(it.M, it.Mp, q < it.nc ? q : 0, N);
             bool stop = false;
@@ -488,10 +503,10 @@ __global__ void __launch_bounds__(kThreads, 1)
                         zr[i] = fma(v.x, cs.x, kMagic);
                         zi[i] = fma(v.y, cs.y, kMagic);
                     }
-                    const int n = 2 * q;   // re row; im is n + 1
-                    unsigned char* unit = Bm + t * kBT + (n >> 3) * 256 + (o >> 1) * 128 + (n & 7) * 16 + (o & 1) * 8;
-                    store_unit8(unit, kBPlane, zr);
-                    store_unit8(unit + 16, kBPlane, zi);
+                    const int n = 16 * t + 2 * q;   // re row of plane 0; im is n + 1; plane p at + 16 nt p
+                    unsigned char* unit = Bm + (n >> 3) * 256 + (o >> 1) * 128 + (n & 7) * 16 + (o & 1) * 8;
+                    store_unit8(unit, 512 * it.nt, zr);
+                    store_unit8(unit + 16, 512 * it.nt, zi);
                 }
                 tc::fence_proxy_async();
                 __syncwarp();
@@ -514,7 +529,7 @@ __global__ void __launch_bounds__(kThreads, 1)
             for (;; ++r) {
                 const int idx = cta_item(r, n_items);
                 if (idx < 0) return -1;
-                if (item_geo<DIR>(groups, segs, nseg, idx).nchunks > 0) return idx;
+                if (item_geo<DIR>(groups, segs, s_first, nseg, idx, hint).nchunks > 0) return idx;
             }
         };
         auto load_scales = [&](const ItemGeo& it, double2& ics, double& rowf) {
@@ -531,7 +546,7 @@ __global__ void __launch_bounds__(kThreads, 1)
         double2 ics_c = make_double2(1.0, 1.0);
         double rowf_c = 0.0;
         if (idx >= 0) {
-            it = item_geo<DIR>(groups, segs, nseg, idx);
+            it = item_geo<DIR>(groups, segs, s_first, nseg, idx, hint);
             load_scales(it, ics_c, rowf_c);
         }
         int n = 0;
@@ -542,7 +557,7 @@ __global__ void __launch_bounds__(kThreads, 1)
             double2 ics_n = make_double2(1.0, 1.0);
             double rowf_n = 0.0;
             if (nidx >= 0) {
-                nit = item_geo<DIR>(groups, segs, nseg, nidx);
+                nit = item_geo<DIR>(groups, segs, s_first, nseg, nidx, hint);
                 load_scales(nit, ics_n, rowf_n);
             }
             const int a = n & 1, ua = n >> 1;
@@ -561,7 +576,7 @@ __global__ void __launch_bounds__(kThreads, 1)
             for (int t = 0; t < it.nt; ++t) {
                 int32_t acc[kPlanes][16];
 #pragma unroll
-                for (int e = 0; e < kPlanes; ++e) tc::tmem_ld16(taddr + (uint32_t)(kAccT * t + 16 * e), acc[e]);
+                for (int e = 0; e < kPlanes; ++e) tc::tmem_ld16(taddr + (uint32_t)(16 * it.nt * e + 16 * t), acc[e]);
                 tc::tmem_wait_ld();
                 double v[16];
 #pragma unroll
@@ -622,87 +637,137 @@ __global__ void __launch_bounds__(kThreads, 1)
             *reinterpret_cast<double2*>(s_cf + 4 * lane + 2) = make_double2(pf1, prs);
             __syncwarp();
         };
-        int g = 0;
-        for (int r = 0;; ++r) {
-            const int idx = cta_item(r, n_items);
-            if (idx < 0 || *s_abort) break;
-            const ItemGeo it = item_geo<DIR>(groups, segs, nseg, idx);
-            const int N = it.N, R = it.R, M = it.M;
-            const DwtGroup* gr = it.gr;
-            const long long rc0 = rc_offset(it.B, it.M, it.Mp);
-            const double nf = gr->normf[it.cls];
-            const double2* rows = aux_of(gr, it.t0) + aux_rows(it.B);
+        // The chunks of this warp, in ring order, with the seed inputs and the first coefficient
+        // batch of the next one loaded while the current one is generated.
+        struct Loc {
+            int r, c, idx;
+            ItemGeo it;
+        };
+        auto locate = [&](Loc& L, int r, int c) {   // the first chunk at or after chunk c of item r
+            for (;;) {
+                L.idx = cta_item(r, n_items);
+                L.r = r;
+                L.c = 0;
+                if (L.idx < 0) return;
+                L.it = item_geo<DIR>(groups, segs, s_first, nseg, L.idx, hint);
+                if (c < L.it.nchunks) {
+                    L.c = c;
+                    return;
+                }
+                c -= L.it.nchunks;
+                ++r;
+            }
+        };
+        struct SeedIn {
+            double cb, wk, nf;
+            double2 ps, pc;
+        };
+        auto load_seed = [&](const Loc& L, SeedIn& si) {
+            si.cb = 0.0;
+            si.wk = 1.0;
+            si.nf = 0.0;
+            si.ps = make_double2(0.0, 0.0);
+            si.pc = make_double2(0.0, 0.0);
+            if (L.idx < 0) return;
+            const DwtGroup* gr = L.it.gr;
+            const int N = L.it.N;
+            const int k = DIR == 0 ? L.c * kKC + lane : 128 * L.it.tile + 32 * w + lane;
+            if (k < N) {
+                si.cb = __ldg(gr->cosb + k);
+                if (DIR == 0) si.wk = __ldg(gr->w + k);
+                si.ps = __ldg(gr->pw_sin + (size_t)(L.it.M - L.it.Mp) * N + k);
+                si.pc = __ldg(gr->pw_cos + (size_t)(L.it.M + L.it.Mp) * N + k);
+            }
+            si.nf = __ldg(gr->normf + L.it.cls);
+        };
+        auto fetch_loc = [&](const Loc& L, int base) {
+            if (L.idx < 0) {
+                pcf = make_double2(0.0, 0.0);
+                pf1 = 0.0;
+                prs = 0.0;
+                return;
+            }
+            fetch(L.it.gr, rc_offset(L.it.B, L.it.M, L.it.Mp), aux_of(L.it.gr, L.it.t0) + aux_rows(L.it.B), L.it.M, L.it.R,
+                  base);
+        };
+        Loc cur;
+        locate(cur, 0, DIR == 0 ? w : 0);
+        int g = DIR == 0 ? w : 0;
+        SeedIn si;
+        load_seed(cur, si);
+        fetch_loc(cur, 0);
+        while (cur.idx >= 0 && !*s_abort) {
+            Loc nx;
+            locate(nx, DIR == 0 ? cur.r : cur.r + 1, DIR == 0 ? cur.c + kGenWarps : 0);
+            SeedIn sn;
+            load_seed(nx, sn);
+            const ItemGeo& it = cur.it;
+            const int N = it.N, R = it.R;
             bool stop = false;
             if (DIR == 0) {
-                // forward: this warp's chunks (beta columns 32c + lane), rows of the item's tile
-                const int r0 = 128 * it.tile, rn = min(R - r0, 128), end = r0 + rn;
-                for (int c = 0; c < it.nchunks; ++c, ++g) {
-                    if ((g % kGenWarps) != w) continue;
-                    const int s = g % kStages, u = g / kStages;
-                    const int k = c * kKC + lane;
-                    double cb = 0.0, dcur = 0.0, dprev = 0.0;
-                    int sc = 0;
-                    if (k < N) {
-                        cb = gr->cosb[k];
-                        dcur = seed_value(nf * gr->w[k], gr->pw_sin[(size_t)(it.M - it.Mp) * N + k],
-                                          gr->pw_cos[(size_t)(it.M + it.Mp) * N + k], sc);
-                    }
-                    bool scaled = __any_sync(0xffffffffu, sc > 0);
-                    fetch(gr, rc0, rows, M, R, 0);
-                    int base = 0;
-                    for (; base < r0; base += 32) {   // second row tile: run through the first 128 degrees
-                        publish();
-                        fetch(gr, rc0, rows, M, R, base + 32);
+                // forward: beta columns 32c + lane of this warp's chunk c, rows of the item's tile
+                const int s = g % kStages, u = g / kStages;
+                const int k = cur.c * kKC + lane;
+                const int r0 = 128 * it.tile, end = r0 + min(R - r0, 128);
+                const double cb = si.cb;
+                double dcur = 0.0, dprev = 0.0;
+                int sc = 0;
+                if (k < N) dcur = seed_value(si.nf * si.wk, si.ps, si.pc, sc);
+                bool scaled = __any_sync(0xffffffffu, sc > 0);
+                int base = 0;
+                for (; base < r0; base += 32) {   // second row tile: run through the first 128 degrees
+                    publish();
+                    fetch_loc(cur, base + 32);
 #pragma unroll 1
-                        for (int h = 0; h < 2; ++h) {
-                            adv16(dcur, dprev, cb, s_cf, 16 * h);
-                            if (scaled) {
-                                rescale_check(dcur, dprev, sc);
-                                scaled = __any_sync(0xffffffffu, sc > 0);
-                            }
+                    for (int h = 0; h < 2; ++h) {
+                        adv16(dcur, dprev, cb, s_cf, 16 * h);
+                        if (scaled) {
+                            rescale_check(dcur, dprev, sc);
+                            scaled = __any_sync(0xffffffffu, sc > 0);
                         }
                     }
-                    if (!tc::mbar_wait_bounded(&bars[kBarEmpty + s], (uint32_t)((u & 1) ^ 1), kWaitNs, s_abort)) {
-                        stop = true;
-                        break;
-                    }
-                    unsigned char* A = smem + s * kStageBytes + lane * 16;   // (k/8)*128 + (k%8)*16 = lane*16
-                    for (; base < end; base += 32) {
-                        publish();
-                        fetch(gr, rc0, rows, M, R, base + 32);
-#pragma unroll 1
-                        for (int h = 0; h < 2; ++h) {
-                            const int b16 = base + 16 * h;
-                            if (b16 >= end) break;
-                            double z[16];
-                            gen16(z, dcur, dprev, sc, cb, s_cf, 16 * h);
-                            if (scaled) {
-                                rescale_check(dcur, dprev, sc);
-                                scaled = __any_sync(0xffffffffu, sc > 0);
-                            }
-                            if (k < N) store_unit16(A + ((b16 - r0) >> 4) * 512, kAPlane, z);
-                        }
-                    }
-                    tc::fence_proxy_async();
-                    __syncwarp();
-                    if (lane == 0) tc::mbar_arrive(&bars[kBarFull + s]);
                 }
+                if (!tc::mbar_wait_bounded(&bars[kBarEmpty + s], (uint32_t)((u & 1) ^ 1), kWaitNs, s_abort)) break;
+                unsigned char* A = smem + s * kStageBytes + lane * 16;   // (k/8)*128 + (k%8)*16 = lane*16
+                for (; base < end; base += 32) {
+                    publish();
+                    if (base + 32 < end)
+                        fetch_loc(cur, base + 32);
+                    else
+                        fetch_loc(nx, 0);
+#pragma unroll 1
+                    for (int h = 0; h < 2; ++h) {
+                        const int b16 = base + 16 * h;
+                        if (b16 >= end) break;
+                        double z[16];
+                        gen16(z, dcur, dprev, sc, cb, s_cf, 16 * h);
+                        if (scaled) {
+                            rescale_check(dcur, dprev, sc);
+                            scaled = __any_sync(0xffffffffu, sc > 0);
+                        }
+                        if (k < N) store_unit16(A + ((b16 - r0) >> 4) * 512, kAPlane, z);
+                    }
+                }
+                tc::fence_proxy_async();
+                __syncwarp();
+                if (lane == 0) tc::mbar_arrive(&bars[kBarFull + s]);
+                g += kGenWarps;
             } else {
                 // inverse: beta column k of the tile for this lane, 32 degrees per chunk
                 const int m = 32 * w + lane;
                 const int k = 128 * it.tile + m;
-                double cb = 0.0, dcur = 0.0, dprev = 0.0;
+                const double cb = si.cb;
+                double dcur = 0.0, dprev = 0.0;
                 int sc = 0;
-                if (k < N) {
-                    cb = gr->cosb[k];
-                    dcur = seed_value(nf, gr->pw_sin[(size_t)(it.M - it.Mp) * N + k], gr->pw_cos[(size_t)(it.M + it.Mp) * N + k], sc);
-                }
+                if (k < N) dcur = seed_value(si.nf, si.ps, si.pc, sc);
                 bool scaled = __any_sync(0xffffffffu, sc > 0);
-                fetch(gr, rc0, rows, M, R, 0);
                 for (int c = 0; c < it.nchunks; ++c, ++g) {
                     const int s = g % kStages, u = g / kStages;
                     publish();
-                    fetch(gr, rc0, rows, M, R, (c + 1) * kKC);
+                    if (c + 1 < it.nchunks)
+                        fetch_loc(cur, (c + 1) * kKC);
+                    else
+                        fetch_loc(nx, 0);
                     if (!tc::mbar_wait_bounded(&bars[kBarEmpty + s], (uint32_t)((u & 1) ^ 1), kWaitNs, s_abort)) {
                         stop = true;
                         break;
@@ -722,8 +787,10 @@ __global__ void __launch_bounds__(kThreads, 1)
                     __syncwarp();
                     if (lane == 0) tc::mbar_arrive(&bars[kBarFull + s]);
                 }
+                if (stop) break;
             }
-            if (stop || *s_abort) break;
+            cur = nx;
+            si = sn;
         }
     }
 
@@ -812,16 +879,21 @@ __global__ void split_inv_prepare_kernel(double2* const* X, const double2* const
         mre = fmax(mre, __shfl_xor_sync(0xffffffffu, mre, o));
         mim = fmax(mim, __shfl_xor_sync(0xffffffffu, mim, o));
     }
-    double2* out = aux + aux_inv(B) + (size_t)inv_chunk_prefix(B, M, Mp) * 256 + q * kKC + lane;
+    double2* blk = aux + aux_inv(B) + (size_t)inv_chunk_prefix(B, M, Mp) * kInvChunk;
 #pragma unroll
     for (int i = 0; i < 8; ++i)
-        if (i < nch) out[(size_t)i * 256] = v[i];
+        if (i < nch) blk[(size_t)i * kInvChunk + kRawHdr / 16 + q * (kRawPitch / 16) + lane] = v[i];
+    double cr, ci, ir, ii;
+    column_scale(mre, cr, ir);
+    column_scale(mim, ci, ii);
+    // the entry goes to the scale table (epilogue) and into the header of each of the class's chunks
     if (lane == 0) {
-        double cr, ci, ir, ii;
-        column_scale(mre, cr, ir);
-        column_scale(mim, ci, ii);
         aux[2 * wid] = make_double2(cr, ci);
         aux[2 * wid + 1] = make_double2(ir, ii);
+    }
+    if (lane < 2 * nch) {
+        double2* h = blk + (size_t)(lane >> 1) * kInvChunk + 2 * q + (lane & 1);
+        *h = (lane & 1) ? make_double2(ir, ii) : make_double2(cr, ci);
     }
 }
 
@@ -858,7 +930,7 @@ bool dwt_split_supported(int B) { return B >= 1 && B <= 256; }
 
 size_t dwt_split_aux_elems(int B)
 {
-    return aux_inv(B) + (size_t)256 * (size_t)inv_chunk_prefix(B, B, 0);
+    return aux_inv(B) + (size_t)kInvChunk * (size_t)inv_chunk_prefix(B, B, 0);
 }
 
 cudaError_t dwt_split_scales(int direction, int B, int T, double2* const* d_ws, const double2* const* d_coeffs,
@@ -891,6 +963,8 @@ int dwt_split_segments(int direction, const std::vector<int>& group, const std::
         sg.group = group[i];
         sg.first = first;
         sg.T = T[i];
+        sg.B = B[i];
+        sg.N = 2 * B[i];
         sg.pairs = (T[i] + kNT - 1) / kNT;
         sg.tiles = direction == 0 ? (B[i] + 127) / 128 : (2 * B[i] + 127) / 128;
         sg.count = num_classes(B[i]) * sg.pairs * sg.tiles;
