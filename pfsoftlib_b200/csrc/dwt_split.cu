@@ -92,14 +92,15 @@ using namespace dwtk;
 constexpr int kNT = 2;                 // transforms per work item (at most)
 constexpr int kPlanes = 6;             // digits per operand
 constexpr int kKC = 32;                // K per chunk: one kind::i8 MMA
-constexpr int kStages = 6;             // operand ring
-constexpr int kRaw = 4;                // raw-data ring
+constexpr int kStages = 5;             // operand ring
+constexpr int kLoadWarps = 3;          // loader warps (bulk copies + digitising)
+constexpr int kRawPerWarp = 2;         // raw slots per loader warp
+constexpr int kRaw = kLoadWarps * kRawPerWarp;
 constexpr int kAccSets = 2;
 constexpr int kAccStride = 256;        // tensor-memory columns between the two accumulator sets
 constexpr uint32_t kTmemCols = 512;
 constexpr int kThreads = 384;
-constexpr int kCopyWarp = 1;
-constexpr int kConvWarp0 = 2, kConvWarps = 2;
+constexpr int kLoadWarp0 = 1;
 constexpr int kEpiWarp0 = 4;
 constexpr int kGenWarp0 = 8, kGenWarps = 4;
 constexpr uint64_t kWaitNs = 2000000000ull;   // 2 s
@@ -122,11 +123,11 @@ constexpr int kOffEpi = kOffCoef + kGenWarps * 32 * 4 * 8;   // epilogue: 16 x {
 constexpr int kSegCache = 256;                      // segment starts kept in shared memory
 constexpr int kOffSeg = kOffEpi + 4 * 16 * 16;     // first item of each segment (the first kSegCache)
 constexpr int kOffBar = kOffSeg + kSegCache * 4;
-// mbarriers: full[kStages], empty[kStages], accfull[2], accempty[2], rawfull[kRaw], rawempty[kRaw],
-// drain, never (test knob)
+// mbarriers: full[kStages], empty[kStages], accfull[2], accempty[2], rawfull[kRaw], drain, never
+// (test knob)
 constexpr int kBarFull = 0, kBarEmpty = kStages, kBarAccFull = 2 * kStages, kBarAccEmpty = 2 * kStages + kAccSets,
-              kBarRawFull = 2 * kStages + 2 * kAccSets, kBarRawEmpty = kBarRawFull + kRaw,
-              kBarDrain = kBarRawEmpty + kRaw, kBarNever = kBarDrain + 1, kNumBars = kBarNever + 1;
+              kBarRawFull = 2 * kStages + 2 * kAccSets, kBarDrain = kBarRawFull + kRaw, kBarNever = kBarDrain + 1,
+              kNumBars = kBarNever + 1;
 constexpr int kOffMisc = kOffBar + kNumBars * 8;    // tensor-memory address, abort flag
 constexpr int kSmemBytes = kOffMisc + 16;
 static_assert(kStageBytes % 1024 == 0, "stages stay 1 KB aligned");
@@ -264,10 +265,70 @@ __device__ __forceinline__ int cta_item(int r, int n_items)
     return i < n_items ? i : -1;
 }
 
+// A chunk of the CTA's ring: chunk c of its r-th item (idx < 0: past the last item).
+struct Loc {
+    int r, c, idx;
+    ItemGeo it;
+};
+
+// The first chunk at or after chunk c of the CTA's r-th item (items without chunks skipped).
+template <int DIR>
+__device__ __forceinline__ void locate(Loc& L, int r, int c, const DwtGroup* __restrict__ groups,
+                                       const SplitSeg* __restrict__ segs, const int* s_first, int nseg, int n_items, int& hint)
+{
+    for (;;) {
+        L.idx = cta_item(r, n_items);
+        L.r = r;
+        L.c = 0;
+        if (L.idx < 0) return;
+        L.it = item_geo<DIR>(groups, segs, s_first, nseg, L.idx, hint);
+        if (c < L.it.nchunks) {
+            L.c = c;
+            return;
+        }
+        c -= L.it.nchunks;
+        ++r;
+    }
+}
+
 __device__ __forceinline__ const double2* aux_of(const DwtGroup* gr, int t)
 {
     const size_t N = (size_t)gr->N;
     return gr->X[t] + N * N * N;
+}
+
+// Loads issued where they stand (volatile: not sunk towards their first use), through the
+// read-only path; the value is waited for only where it is first used.
+__device__ __forceinline__ double ld_early(const double* p)
+{
+    double v;
+    asm volatile("ld.global.nc.f64 %0, [%1];" : "=d"(v) : "l"(p));
+    return v;
+}
+__device__ __forceinline__ double2 ld_early(const double2* p)
+{
+    double2 v;
+    asm volatile("ld.global.nc.v2.f64 {%0, %1}, [%2];" : "=d"(v.x), "=d"(v.y) : "l"(p));
+    return v;
+}
+
+// seed_value (dwt_common.cuh) with frexp / ldexp done on the bit pattern: the same value and scale
+// count. The product of normal table mantissas is normal; a zero product gives 0 (unscaled).
+__device__ __forceinline__ double seed_bits(double nf_w, double2 s, double2 c, int& sc)
+{
+    const double x = nf_w * s.x * c.x;
+    const unsigned long long bits = (unsigned long long)__double_as_longlong(x);
+    const int ef = (int)((bits >> 52) & 0x7FF);
+    sc = 0;
+    if (ef == 0) return x == 0.0 ? 0.0 : seed_value(nf_w, s, c, sc);
+    const int E = ef - 1022 + (int)s.y + (int)c.y;   // frexp exponent of x plus the table exponents
+    int Eo = E;
+    if (E < -900) {
+        sc = (-900 - E + 599) / 600;
+        Eo = E + 600 * sc;
+    }
+    const unsigned long long r = (bits & ~(0x7FFull << 52)) | ((unsigned long long)(1022 + Eo) << 52);
+    return -__longlong_as_double((long long)r);
 }
 
 // One recurrence step of a beta column (fn_dwt.hpp:167-199): d(l+1) = d(l)(f1 f2 + f1 cos b) + c1 d(l-1).
@@ -340,10 +401,7 @@ __global__ void __launch_bounds__(kThreads, 1)
             tc::mbar_init(&bars[kBarAccFull + a], 1);
             tc::mbar_init(&bars[kBarAccEmpty + a], 4);   // the four epilogue warps
         }
-        for (int r = 0; r < kRaw; ++r) {
-            tc::mbar_init(&bars[kBarRawFull + r], 1);    // arrive.expect_tx of the copy warp + the bytes
-            tc::mbar_init(&bars[kBarRawEmpty + r], 1);   // the digitising warp
-        }
+        for (int r = 0; r < kRaw; ++r) tc::mbar_init(&bars[kBarRawFull + r], 1);   // arrive.expect_tx + the bytes
         tc::mbar_init(&bars[kBarDrain], 1);
         tc::mbar_init(&bars[kBarNever], 1);
         tc::mbar_fence_init();
@@ -406,116 +464,122 @@ __global__ void __launch_bounds__(kThreads, 1)
                 if (tc::globaltimer_ns() - t0 > kWaitNs) break;
         }
         __syncwarp();
-    } else if (warp == kCopyWarp) {
-        // ------------------------------------------------------------------ bulk copies (data operand)
-        // lane i < 9 nt: transform i / 9, entry j = i % 9: j < 8 the 32 values of case j, j = 8 the
-        // transform's 8 scale entries
-        int g = 0;
-        for (int r = 0;; ++r) {
-            const int idx = cta_item(r, n_items);
-            if (idx < 0 || *s_abort) break;
-            const ItemGeo it = item_geo<DIR>(groups, segs, s_first, nseg, idx, hint);
-            const int N = it.N;
-            const int t = lane / 9, j = lane - 9 * (lane / 9);
-            const bool tl = t < it.nt;
-            const double2* aux = aux_of(it.gr, it.t0 + (tl ? t : 0));
-            PairCase p = class_case(it.M, it.Mp, (j < it.nc && j < 8) ? j : 0, N);
-            const long long ib = DIR == 1 ? inv_chunk_prefix(it.B, it.M, it.Mp) : 0;
-            bool stop = false;
-            for (int c = 0; c < it.nchunks; ++c, ++g) {
-                const int slot = g % kRaw, u = g / kRaw;
-                if (!tc::mbar_wait_bounded(&bars[kBarRawEmpty + slot], (uint32_t)((u & 1) ^ 1), kWaitNs, s_abort)) {
-                    stop = true;
-                    break;
-                }
-                const int len = min(kKC, N - kKC * c);   // forward: beta samples of this chunk
-                const uint32_t per_t = DIR == 0 ? (uint32_t)(kRawHdr + it.nc * len * 16) : (uint32_t)kRawT;
-                if (lane == 0) tc::mbar_arrive_expect_tx(&bars[kBarRawFull + slot], per_t * (uint32_t)it.nt);
-                __syncwarp();
-                unsigned char* dst = smem + kOffRaw + slot * kRawBytes + t * kRawT;
-                if (DIR == 1) {
-                    // the chunk block of transform t (lane t < nt): header and data in one copy
-                    if (lane < it.nt)
-                        tc::bulk_g2s(smem + kOffRaw + slot * kRawBytes + lane * kRawT,
-                                     aux_of(it.gr, it.t0 + lane) + aux_inv(it.B) + (size_t)(ib + c) * kInvChunk, (uint32_t)kRawT,
-                                     &bars[kBarRawFull + slot]);
-                } else if (tl && j == 8) {
-                    tc::bulk_g2s(dst, aux + (size_t)2 * 8 * it.cls, kRawHdr, &bars[kBarRawFull + slot]);
-                } else if (tl && j < 8) {
-                    if (j < it.nc) {
+    } else if (warp >= kLoadWarp0 && warp < kLoadWarp0 + kLoadWarps) {
+        // ------------------------------------------------------------------ loaders (data operand)
+        // Warp L takes chunks g = L + 3j of the ring; its two raw slots alternate (chunk j in slot
+        // 2L + j%2). The bulk copies of chunk j+2 are issued as soon as chunk j has been digitised,
+        // so two chunks of copies per warp are in flight (several issuing warps: one warp issuing
+        // many small copies is the slower path). Digitising: lane = 8 o + q, case q, beta / degree
+        // octet o of the chunk (a quarter warp reads the eight cases of one octet: distinct banks).
+        const int L = warp - kLoadWarp0;
+        const int q = lane & 7, o = lane >> 3;
+        auto issue = [&](const Loc& Lc, int sl) {
+            if (Lc.idx < 0) return;
+            const ItemGeo& it = Lc.it;
+            const int c = Lc.c, N = it.N;
+            unsigned char* base = smem + kOffRaw + sl * kRawBytes;
+            uint64_t* bar = &bars[kBarRawFull + sl];
+            const int len = min(kKC, N - kKC * c);   // forward: beta samples of this chunk
+            const uint32_t per_t = DIR == 0 ? (uint32_t)(kRawHdr + it.nc * len * 16) : (uint32_t)kRawT;
+            tc::fence_proxy_async();   // this warp's reads of the slot come before the copies into it
+            if (lane == 0) tc::mbar_arrive_expect_tx(bar, per_t * (uint32_t)it.nt);
+            __syncwarp();
+            if (DIR == 1) {
+                // the chunk block of transform `lane`: header and data in one copy
+                if (lane < it.nt)
+                    tc::bulk_g2s(base + lane * kRawT,
+                                 aux_of(it.gr, it.t0 + lane) + aux_inv(it.B) +
+                                     (size_t)(inv_chunk_prefix(it.B, it.M, it.Mp) + c) * kInvChunk,
+                                 (uint32_t)kRawT, bar);
+            } else {
+                // lane 9 t + j: j < 8 the chunk of case j's bin column, j = 8 the scale header
+                const int t = lane / 9, j = lane - 9 * (lane / 9);
+                if (t < it.nt) {
+                    if (j == 8) {
+                        tc::bulk_g2s(base + t * kRawT, aux_of(it.gr, it.t0 + t) + (size_t)2 * 8 * it.cls, kRawHdr, bar);
+                    } else if (j < it.nc) {
+                        const PairCase p = class_case(it.M, it.Mp, j, N);
                         const int k0 = p.rev ? N - kKC * c - len : kKC * c;
-                        tc::bulk_g2s(dst + kRawHdr + j * kRawPitch,
-                                     it.gr->X[it.t0 + t] + ((size_t)p.row * N + p.col) * N + k0, (uint32_t)len * 16u,
-                                     &bars[kBarRawFull + slot]);
+                        tc::bulk_g2s(base + t * kRawT + kRawHdr + j * kRawPitch,
+                                     it.gr->X[it.t0 + t] + ((size_t)p.row * N + p.col) * N + k0, (uint32_t)len * 16u, bar);
                     }
                 }
-                __syncwarp();
             }
-            if (stop || *s_abort) break;
+            __syncwarp();
+        };
+        int nis0 = 0, nis1 = 0;   // copies issued into this warp's two slots
+        Loc cur, nxt;
+        locate<DIR>(cur, 0, L, groups, segs, s_first, nseg, n_items, hint);
+        nxt.idx = -1;
+        if (cur.idx >= 0) locate<DIR>(nxt, cur.r, cur.c + kLoadWarps, groups, segs, s_first, nseg, n_items, hint);
+        if (cur.idx >= 0) {
+            issue(cur, kRawPerWarp * L);
+            ++nis0;
         }
-        // the copies of the last armed phase of each slot have landed before the CTA can end
-        for (int k = 1; k <= kRaw && g - k >= 0; ++k) {
-            const int gg = g - k;
-            const uint64_t t0 = tc::globaltimer_ns();
-            while (!tc::mbar_try_wait(&bars[kBarRawFull + gg % kRaw], (uint32_t)((gg / kRaw) & 1)))
-                if (tc::globaltimer_ns() - t0 > kWaitNs) break;
+        if (nxt.idx >= 0) {
+            issue(nxt, kRawPerWarp * L + 1);
+            ++nis1;
         }
-    } else if (warp >= kConvWarp0 && warp < kConvWarp0 + kConvWarps) {
-        // ------------------------------------------------------------------ digitise the data operand
-        // lane = 8 o + q: case q, beta / degree octet o of the chunk (a quarter warp reads the
-        // eight cases of one octet: distinct bank groups)
-        const int L = warp - kConvWarp0;
-        const int q = lane & 7, o = lane >> 3;
-        int g = 0;
-        for (int r = 0;; ++r) {
-            const int idx = cta_item(r, n_items);
-            if (idx < 0 || *s_abort) break;
-            const ItemGeo it = item_geo<DIR>(groups, segs, s_first, nseg, idx, hint);
+        int g = L;
+        for (int j = 0; cur.idx >= 0 && !*s_abort; ++j) {
+            const int sl = kRawPerWarp * L + (j & 1);
+            const int s = g % kStages, us = g / kStages;
+            if (!tc::mbar_wait_bounded(&bars[kBarRawFull + sl], (uint32_t)((j >> 1) & 1), kWaitNs, s_abort) ||
+                !tc::mbar_wait_bounded(&bars[kBarEmpty + s], (uint32_t)((us & 1) ^ 1), kWaitNs, s_abort))
+                break;
+            const ItemGeo& it = cur.it;
             const int N = it.N;
             const PairCase p = class_case(it.M, it.Mp, q < it.nc ? q : 0, N);
-            bool stop = false;
-            for (int c = 0; c < it.nchunks; ++c, ++g) {
-                if ((g % kConvWarps) != L) continue;
-                const int slot = g % kRaw, u = g / kRaw;
-                const int s = g % kStages, us = g / kStages;
-                if (!tc::mbar_wait_bounded(&bars[kBarRawFull + slot], (uint32_t)(u & 1), kWaitNs, s_abort) ||
-                    !tc::mbar_wait_bounded(&bars[kBarEmpty + s], (uint32_t)((us & 1) ^ 1), kWaitNs, s_abort)) {
-                    stop = true;
-                    break;
-                }
-                const unsigned char* raw = smem + kOffRaw + slot * kRawBytes;
-                unsigned char* Bm = smem + s * kStageBytes + kABytes;
-                const int len = min(kKC, N - kKC * c);
-                for (int t = 0; t < it.nt; ++t) {
-                    if (q >= it.nc) continue;   // rows of absent cases are never read back
-                    const double2 cs = *reinterpret_cast<const double2*>(raw + t * kRawT + 32 * q);
-                    const double2* col = reinterpret_cast<const double2*>(raw + t * kRawT + kRawHdr + q * kRawPitch);
-                    double zr[8], zi[8];
+            const unsigned char* raw = smem + kOffRaw + sl * kRawBytes;
+            unsigned char* Bm = smem + s * kStageBytes + kABytes;
+            const int len = min(kKC, N - kKC * cur.c);
+            for (int t = 0; t < it.nt; ++t) {
+                if (q >= it.nc) continue;   // rows of absent cases are never read back
+                const double2 cs = *reinterpret_cast<const double2*>(raw + t * kRawT + 32 * q);
+                const double2* col = reinterpret_cast<const double2*>(raw + t * kRawT + kRawHdr + q * kRawPitch);
+                double zr[8], zi[8];
 #pragma unroll
-                    for (int i = 0; i < 8; ++i) {
-                        const int kk = 8 * o + i;   // position in the chunk
-                        double2 v = make_double2(0.0, 0.0);
-                        if (DIR == 0) {
-                            if (kk < len) v = col[p.rev ? len - 1 - kk : kk];
-                        } else {
-                            v = col[kk];   // zero past the class's last degree
-                        }
-                        zr[i] = fma(v.x, cs.x, kMagic);
-                        zi[i] = fma(v.y, cs.y, kMagic);
+                for (int i = 0; i < 8; ++i) {
+                    const int kk = 8 * o + i;   // position in the chunk
+                    double2 v = make_double2(0.0, 0.0);
+                    if (DIR == 0) {
+                        if (kk < len) v = col[p.rev ? len - 1 - kk : kk];
+                    } else {
+                        v = col[kk];   // zero past the class's last degree
                     }
-                    const int n = 16 * t + 2 * q;   // re row of plane 0; im is n + 1; plane p at + 16 nt p
-                    unsigned char* unit = Bm + (n >> 3) * 256 + (o >> 1) * 128 + (n & 7) * 16 + (o & 1) * 8;
-                    store_unit8(unit, 512 * it.nt, zr);
-                    store_unit8(unit + 16, 512 * it.nt, zi);
+                    zr[i] = fma(v.x, cs.x, kMagic);
+                    zi[i] = fma(v.y, cs.y, kMagic);
                 }
-                tc::fence_proxy_async();
-                __syncwarp();
-                if (lane == 0) {
-                    tc::mbar_arrive(&bars[kBarFull + s]);
-                    tc::mbar_arrive(&bars[kBarRawEmpty + slot]);
-                }
+                const int n = 16 * t + 2 * q;   // re row of plane 0; im is n + 1; plane p at + 16 nt p
+                unsigned char* unit = Bm + (n >> 3) * 256 + (o >> 1) * 128 + (n & 7) * 16 + (o & 1) * 8;
+                store_unit8(unit, 512 * it.nt, zr);
+                store_unit8(unit + 16, 512 * it.nt, zi);
             }
-            if (stop || *s_abort) break;
+            tc::fence_proxy_async();
+            __syncwarp();
+            if (lane == 0) tc::mbar_arrive(&bars[kBarFull + s]);
+            // chunk j + 2 of this warp into the slot just read
+            Loc n2;
+            n2.idx = -1;
+            if (nxt.idx >= 0) locate<DIR>(n2, nxt.r, nxt.c + kLoadWarps, groups, segs, s_first, nseg, n_items, hint);
+            if (n2.idx >= 0) {
+                issue(n2, sl);
+                if (j & 1)
+                    ++nis1;
+                else
+                    ++nis0;
+            }
+            cur = nxt;
+            nxt = n2;
+            g += kLoadWarps;
+        }
+        // the copies of each slot's last armed phase have landed before the CTA can end
+        for (int k = 0; k < kRawPerWarp; ++k) {
+            const int ni = k == 0 ? nis0 : nis1;
+            if (ni == 0) continue;
+            const uint64_t t0 = tc::globaltimer_ns();
+            while (!tc::mbar_try_wait(&bars[kBarRawFull + kRawPerWarp * L + k], (uint32_t)((ni - 1) & 1)))
+                if (tc::globaltimer_ns() - t0 > kWaitNs) break;
         }
     } else if (warp >= kEpiWarp0 && warp < kEpiWarp0 + 4) {
         // ------------------------------------------------------------------ epilogue
@@ -535,10 +599,10 @@ __global__ void __launch_bounds__(kThreads, 1)
         auto load_scales = [&](const ItemGeo& it, double2& ics, double& rowf) {
             const int t = lane >> 3, q = lane & 7;
             ics = make_double2(1.0, 1.0);
-            if (lane < 16 && t < it.nt && q < it.nc) ics = __ldg(aux_of(it.gr, it.t0 + t) + (size_t)2 * (8 * it.cls + q) + 1);
+            if (lane < 16 && t < it.nt && q < it.nc) ics = ld_early(aux_of(it.gr, it.t0 + t) + (size_t)2 * (8 * it.cls + q) + 1);
             rowf = 0.0;
             const int l = it.M + 128 * it.tile + row;
-            if (DIR == 0 && l < it.B) rowf = (kPi / (double)(it.B * 2 * it.B)) * __ldg(&aux_of(it.gr, it.t0)[aux_rows(it.B) + l].y);   // src/fn_dsoft.cpp:119
+            if (DIR == 0 && l < it.B) rowf = ld_early(&aux_of(it.gr, it.t0)[aux_rows(it.B) + l].y);
         };
         int r = 0;
         int idx = next_item(r);
@@ -593,7 +657,7 @@ __global__ void __launch_bounds__(kThreads, 1)
                     const PairCase p = class_case(it.M, it.Mp, q, N);
                     const double2 ics = s_ics[8 * t + q];
                     if (DIR == 0) {
-                        const double f = rowf_c * case_sign(p, l, it.M);
+                        const double f = (kPi / (double)(B * 2 * B)) * rowf_c * case_sign(p, l, it.M);   // src/fn_dsoft.cpp:119
                         it.gr->coeffs[it.t0 + t][coef_index(l, p.m1, p.m2)] =
                             make_double2(f * v[2 * q] * ics.x, f * v[2 * q + 1] * ics.y);
                     } else {
@@ -626,9 +690,9 @@ __global__ void __launch_bounds__(kThreads, 1)
             pf1 = 0.0;
             prs = 0.0;
             if (rr < R) {
-                pcf = __ldg(gr->rc_cf + rc0 + rr);
-                pf1 = __ldg(gr->rc_f1 + rc0 + rr);
-                prs = __ldg(&rows[M + rr].x);
+                pcf = ld_early(gr->rc_cf + rc0 + rr);
+                pf1 = ld_early(gr->rc_f1 + rc0 + rr);
+                prs = ld_early(&rows[M + rr].x);
             }
         };
         auto publish = [&]() {
@@ -639,25 +703,7 @@ __global__ void __launch_bounds__(kThreads, 1)
         };
         // The chunks of this warp, in ring order, with the seed inputs and the first coefficient
         // batch of the next one loaded while the current one is generated.
-        struct Loc {
-            int r, c, idx;
-            ItemGeo it;
-        };
-        auto locate = [&](Loc& L, int r, int c) {   // the first chunk at or after chunk c of item r
-            for (;;) {
-                L.idx = cta_item(r, n_items);
-                L.r = r;
-                L.c = 0;
-                if (L.idx < 0) return;
-                L.it = item_geo<DIR>(groups, segs, s_first, nseg, L.idx, hint);
-                if (c < L.it.nchunks) {
-                    L.c = c;
-                    return;
-                }
-                c -= L.it.nchunks;
-                ++r;
-            }
-        };
+        auto locate_g = [&](Loc& L, int r, int c) { locate<DIR>(L, r, c, groups, segs, s_first, nseg, n_items, hint); };
         struct SeedIn {
             double cb, wk, nf;
             double2 ps, pc;
@@ -673,12 +719,12 @@ __global__ void __launch_bounds__(kThreads, 1)
             const int N = L.it.N;
             const int k = DIR == 0 ? L.c * kKC + lane : 128 * L.it.tile + 32 * w + lane;
             if (k < N) {
-                si.cb = __ldg(gr->cosb + k);
-                if (DIR == 0) si.wk = __ldg(gr->w + k);
-                si.ps = __ldg(gr->pw_sin + (size_t)(L.it.M - L.it.Mp) * N + k);
-                si.pc = __ldg(gr->pw_cos + (size_t)(L.it.M + L.it.Mp) * N + k);
+                si.cb = ld_early(gr->cosb + k);
+                if (DIR == 0) si.wk = ld_early(gr->w + k);
+                si.ps = ld_early(gr->pw_sin + (size_t)(L.it.M - L.it.Mp) * N + k);
+                si.pc = ld_early(gr->pw_cos + (size_t)(L.it.M + L.it.Mp) * N + k);
             }
-            si.nf = __ldg(gr->normf + L.it.cls);
+            si.nf = ld_early(gr->normf + L.it.cls);
         };
         auto fetch_loc = [&](const Loc& L, int base) {
             if (L.idx < 0) {
@@ -691,14 +737,14 @@ __global__ void __launch_bounds__(kThreads, 1)
                   base);
         };
         Loc cur;
-        locate(cur, 0, DIR == 0 ? w : 0);
+        locate_g(cur, 0, DIR == 0 ? w : 0);
         int g = DIR == 0 ? w : 0;
         SeedIn si;
         load_seed(cur, si);
         fetch_loc(cur, 0);
         while (cur.idx >= 0 && !*s_abort) {
             Loc nx;
-            locate(nx, DIR == 0 ? cur.r : cur.r + 1, DIR == 0 ? cur.c + kGenWarps : 0);
+            locate_g(nx, DIR == 0 ? cur.r : cur.r + 1, DIR == 0 ? cur.c + kGenWarps : 0);
             SeedIn sn;
             load_seed(nx, sn);
             const ItemGeo& it = cur.it;
@@ -712,7 +758,7 @@ __global__ void __launch_bounds__(kThreads, 1)
                 const double cb = si.cb;
                 double dcur = 0.0, dprev = 0.0;
                 int sc = 0;
-                if (k < N) dcur = seed_value(si.nf * si.wk, si.ps, si.pc, sc);
+                if (k < N) dcur = seed_bits(si.nf * si.wk, si.ps, si.pc, sc);
                 bool scaled = __any_sync(0xffffffffu, sc > 0);
                 int base = 0;
                 for (; base < r0; base += 32) {   // second row tile: run through the first 128 degrees
@@ -759,7 +805,7 @@ __global__ void __launch_bounds__(kThreads, 1)
                 const double cb = si.cb;
                 double dcur = 0.0, dprev = 0.0;
                 int sc = 0;
-                if (k < N) dcur = seed_value(si.nf, si.ps, si.pc, sc);
+                if (k < N) dcur = seed_bits(si.nf, si.ps, si.pc, sc);
                 bool scaled = __any_sync(0xffffffffu, sc > 0);
                 for (int c = 0; c < it.nchunks; ++c, ++g) {
                     const int s = g % kStages, u = g / kStages;
