@@ -347,6 +347,16 @@ int get_tables(int B, cudaStream_t stream, BandTables* out)
         e = tables_build(B, mem, &t, stream);
     }
     if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
+    if (e == cudaSuccess && fft_needs_bluestein(2 * B)) {
+        // lengths with a large prime factor: the FFT's Bluestein table, computed on the host
+        std::vector<double2> h(fft_bluestein_elems(2 * B));
+        fft_bluestein_fill(2 * B, h.data());
+        void* bt = nullptr;
+        e = cudaMalloc(&bt, h.size() * sizeof(double2));
+        if (e == cudaSuccess) e = cudaMemcpy(bt, h.data(), h.size() * sizeof(double2), cudaMemcpyHostToDevice);
+        if (e == cudaSuccess) t.bluestein = static_cast<double2*>(bt);
+        else if (bt) cudaFree(bt);
+    }
     if (e != cudaSuccess) {
         cudaFree(mem);
         return cuda_fail(e, "tables_build");
@@ -399,6 +409,7 @@ FftPassArgs pass_args(int n, int nvec, const BandTables& t, FftStrides src, FftS
     a.dst = dst;
     a.scale = scale;
     a.twiddle = t.twiddle;
+    a.bluestein = t.bluestein;
     return a;
 }
 
@@ -689,11 +700,14 @@ static int layer_wise(int cols, int rows, int lays, double* d_arr, double scale,
         const int n = lens[pass];
         const double2* tw = nullptr;
         void* tmp = nullptr;
+        const double2* blu = nullptr;
+        void* tmp_b = nullptr;
         if (n % 2 == 0 && valid_bandwidth(n / 2)) {
             BandTables t;
             int rc = get_tables(n / 2, s, &t);
             if (rc) return rc;
             tw = t.twiddle;
+            blu = t.bluestein;
         } else {
             // odd length: a private table (rare); freed after the stream drains
             std::vector<double2> h(n);
@@ -705,6 +719,13 @@ static int layer_wise(int cols, int rows, int lays, double* d_arr, double scale,
             PF_CUDA(cudaMemcpyAsync(tmp, h.data(), n * sizeof(double2), cudaMemcpyHostToDevice, s));
             PF_CUDA(cudaStreamSynchronize(s));
             tw = static_cast<const double2*>(tmp);
+            if (fft_needs_bluestein(n)) {
+                std::vector<double2> hb(fft_bluestein_elems(n));
+                fft_bluestein_fill(n, hb.data());
+                PF_CUDA(cudaMalloc(&tmp_b, hb.size() * sizeof(double2)));
+                PF_CUDA(cudaMemcpy(tmp_b, hb.data(), hb.size() * sizeof(double2), cudaMemcpyHostToDevice));
+                blu = static_cast<const double2*>(tmp_b);
+            }
         }
         FftPassArgs a;
         memset(&a, 0, sizeof(a));
@@ -712,6 +733,7 @@ static int layer_wise(int cols, int rows, int lays, double* d_arr, double scale,
         a.kb = fft_tile_vectors(n);
         a.nstages = fft_plan_radices(n, a.radix, a.ns);
         a.twiddle = tw;
+        a.bluestein = blu;
         a.scale = pass == 1 ? scale : 1.0;
         int ntiles;
         if (pass == 0) {
@@ -733,9 +755,10 @@ static int layer_wise(int cols, int rows, int lays, double* d_arr, double scale,
             double2* base = G + (long long)t0 * a.src.sb;
             e = fft_pass_launch(base, base, a, nt, sign, s);
         }
-        if (tmp) {
+        if (tmp || tmp_b) {
             cudaStreamSynchronize(s);
             cudaFree(tmp);
+            cudaFree(tmp_b);
         }
         if (e != cudaSuccess) return cuda_fail(e, "fft_pass_launch");
     }

@@ -91,6 +91,7 @@ FftPassArgs group_pass_args(int dir, bool first, const BandTables& t, double2** 
     a.kb = fft_tile_vectors(t.N);
     a.nstages = fft_plan_radices(t.N, a.radix, a.ns);
     a.twiddle = t.twiddle;
+    a.bluestein = t.bluestein;
     a.scale = 1.0;
     if (dir == 0 && first) {          // F1
         a.src = FftStrides{n2, n, 1};

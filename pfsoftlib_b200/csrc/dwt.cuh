@@ -24,6 +24,7 @@ struct BandTables {
     double2* rc_cf = nullptr;
     double* rc_f1 = nullptr;
     void* block = nullptr;      // single allocation holding all of the above
+    double2* bluestein = nullptr;   // N with a prime factor above 16: the FFT's Bluestein table (own allocation)
 };
 
 // Entries of the recurrence-coefficient table before class (M, M'): classes run M = 0, 1, ...

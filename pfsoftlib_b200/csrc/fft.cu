@@ -16,7 +16,9 @@
 // (alpha, gamma) transpose rides inside the first and last stage at no extra HBM traffic.
 
 #include <algorithm>
+#include <cmath>
 #include <cstring>
+#include <vector>
 
 #include "common.cuh"
 #include "fft.cuh"
@@ -341,7 +343,10 @@ __global__ void __launch_bounds__(256, 4) fft_pass_inplace_kernel(const double2*
 }
 
 
-// Direct O(R^2) butterfly for any other radix (rare lengths with a large prime factor).
+// Direct O(R^2) butterfly for any other radix (lengths with a prime factor above 5). The stage's
+// outputs, not its butterflies, are spread over the threads: a large prime leaves few butterflies
+// per tile (m = n / R of them per vector), while each of the R outputs of a butterfly is an
+// independent R-term sum. A stage never writes the buffer it reads.
 template <int SIGN>
 __device__ void run_stage_generic(const FftPassArgs& a, int s, const double2* gsrc,
                                   double2* gdst, const double2* sin_, double2* sout, int nv,
@@ -355,31 +360,38 @@ __device__ void run_stage_generic(const FftPassArgs& a, int s, const double2* gs
     const bool first = (s == 0), last = (s == a.nstages - 1);
     const int pl = padded_len(n);
     const bool kk_fast = (first && a.src.se != 1) || (last && a.dst.se != 1);
-    const int total = nv * m;
+    const int total = nv * m * R;
     for (int t = threadIdx.x; t < total; t += blockDim.x) {
-        int j, kk;
-        if (kk_fast) {
+        int j, kk, q;
+        if (kk_fast) {   // consecutive threads: consecutive vectors (contiguous in HBM)
             kk = t % nv;
-            j = t / nv;
+            const int u = t / nv;
+            q = u % R;
+            j = u / R;
         } else {
-            j = t % m;
-            kk = t / m;
+            q = t % R;
+            const int u = t / R;
+            j = u % m;
+            kk = u / m;
         }
         const int k = j % Ns;
         const int ob = (j / Ns) * Ns * R + k;
-        for (int q = 0; q < R; ++q) {
-            double2 acc = make_double2(0.0, 0.0);
-            for (int r = 0; r < R; ++r) {
-                double2 x = first ? load_src(a, gsrc + src_base + (long long)kk * a.src.sv + (long long)(j + r * m) * a.src.se)
-                                  : sin_[kk * pl + spos(j + r * m)];
-                if (Ns > 1 && r > 0) x = cmul(x, twiddle(a.twiddle, r * k * step, SIGN));
-                const int e = (r * q) % R;
-                if (e) x = cmul(x, twiddle(a.twiddle, e * rstep, SIGN));
-                acc = cadd(acc, x);
-            }
-            if (last) gdst[dst_base + (long long)kk * a.dst.sv + (long long)(ob + q * Ns) * a.dst.se] = cscale(acc, a.scale);
-            else sout[kk * pl + spos(ob + q * Ns)] = acc;
+        // input r carries the stage twiddle w_n^(r k step) and the DFT twiddle w_R^(r q) =
+        // w_n^(r q rstep): one table entry w_n^(r cq mod n), its index advanced by cq per input
+        const int cq = (int)(((long long)k * step + (long long)q * rstep) % n);
+        double2 acc = first ? load_src(a, gsrc + src_base + (long long)kk * a.src.sv + (long long)j * a.src.se)
+                            : sin_[kk * pl + spos(j)];
+        int e = 0;
+        for (int r = 1; r < R; ++r) {
+            double2 x = first ? load_src(a, gsrc + src_base + (long long)kk * a.src.sv + (long long)(j + r * m) * a.src.se)
+                              : sin_[kk * pl + spos(j + r * m)];
+            e += cq;
+            if (e >= n) e -= n;
+            if (e) x = cmul(x, twiddle(a.twiddle, e, SIGN));
+            acc = cadd(acc, x);
         }
+        if (last) gdst[dst_base + (long long)kk * a.dst.sv + (long long)(ob + q * Ns) * a.dst.se] = cscale(acc, a.scale);
+        else sout[kk * pl + spos(ob + q * Ns)] = acc;
     }
 }
 
@@ -555,6 +567,92 @@ __global__ void __launch_bounds__(256, Tile::kMinBlocks) fft_fused_kernel(const 
     }
 }
 
+// Bluestein pass: kBluesteinVec vectors per CTA, each loaded, multiplied by its chirp and
+// zero-padded to M in shared memory, transformed (radix-2, decimation in frequency: natural order
+// in, bit-reversed out), multiplied by the bit-reversed transform of the chirp kernel (1/M
+// included), transformed back (decimation in time: bit-reversed in, natural out), multiplied by
+// the chirp and stored. The same HBM access pattern as a pass kernel's first and last stages.
+constexpr int kBluesteinVec = 4;
+
+template <int SIGN>
+__global__ void __launch_bounds__(256) fft_bluestein_kernel(const double2* src, double2* dst, const FftPassArgs a, int M)
+{
+    extern __shared__ double2 smem[];   // [kBluesteinVec][M]
+    if (a.srcs) {
+        src = a.srcs[blockIdx.z];
+        dst = a.dsts[blockIdx.z];
+    }
+    const int n = a.n, half = M >> 1;
+    const double2* wtab = a.bluestein;                                 // exp(-pi i e^2 / n)
+    const double2* fh = a.bluestein + n + (SIGN < 0 ? 0 : M);          // bit-reversed, 1/M included
+    const double2* tw = a.bluestein + n + 2 * M;                       // exp(-2 pi i t / M), t < M/2
+    const int v0 = blockIdx.x * kBluesteinVec;
+    const int nv = min(kBluesteinVec, a.nvec - v0);
+    const long long sbase = (long long)v0 * a.src.sv + (long long)blockIdx.y * a.src.sb;
+    const long long dbase = (long long)v0 * a.dst.sv + (long long)blockIdx.y * a.dst.sb;
+    const bool vfast_in = a.src.se != 1, vfast_out = a.dst.se != 1;   // vectors contiguous in HBM
+    for (int t = threadIdx.x; t < kBluesteinVec * M; t += blockDim.x) {
+        int v, e;
+        if (vfast_in) {
+            v = t % kBluesteinVec;
+            e = t / kBluesteinVec;
+        } else {
+            e = t & (M - 1);
+            v = t / M;
+        }
+        double2 x = make_double2(0.0, 0.0);
+        if (v < nv && e < n) {
+            double2 w = wtab[e];
+            if (SIGN > 0) w.y = -w.y;
+            x = cmul(load_src(a, src + sbase + (long long)v * a.src.sv + (long long)e * a.src.se), w);
+        }
+        smem[v * M + e] = x;
+    }
+    __syncthreads();
+    for (int span = half; span >= 1; span >>= 1) {
+        const int tstep = half / span;
+        for (int b = threadIdx.x; b < kBluesteinVec * half; b += blockDim.x) {
+            const int v = b / half, i2 = b - v * half;
+            const int blk = i2 / span, i = i2 - blk * span;
+            const int p = v * M + blk * 2 * span + i, q = p + span;
+            const double2 u = smem[p], x = smem[q];
+            smem[p] = cadd(u, x);
+            smem[q] = cmul(csub(u, x), tw[i * tstep]);
+        }
+        __syncthreads();
+    }
+    for (int t = threadIdx.x; t < kBluesteinVec * M; t += blockDim.x) smem[t] = cmul(smem[t], fh[t & (M - 1)]);
+    __syncthreads();
+    for (int span = 1; span <= half; span <<= 1) {
+        const int tstep = half / span;
+        for (int b = threadIdx.x; b < kBluesteinVec * half; b += blockDim.x) {
+            const int v = b / half, i2 = b - v * half;
+            const int blk = i2 / span, i = i2 - blk * span;
+            const int p = v * M + blk * 2 * span + i, q = p + span;
+            double2 w = tw[i * tstep];
+            w.y = -w.y;
+            const double2 u = smem[p], x = cmul(smem[q], w);
+            smem[p] = cadd(u, x);
+            smem[q] = csub(u, x);
+        }
+        __syncthreads();
+    }
+    for (int t = threadIdx.x; t < kBluesteinVec * n; t += blockDim.x) {
+        int v, k;
+        if (vfast_out) {
+            v = t % kBluesteinVec;
+            k = t / kBluesteinVec;
+        } else {
+            k = t % n;
+            v = t / n;
+        }
+        if (v >= nv) continue;
+        double2 w = wtab[k];
+        if (SIGN > 0) w.y = -w.y;
+        dst[dbase + (long long)v * a.dst.sv + (long long)k * a.dst.se] = cscale(cmul(smem[v * M + k], w), a.scale);
+    }
+}
+
 // Lengths that run the in-place kernel: tile vectors and radices (0 ends a shorter plan). 384 is
 // planned 8.4.4.3 rather than 16.8.3: radix 16 does not fit the kernel's 64 registers. Measured
 // and left on the ping-pong kernel: 256 as 8.8.4 (125 against 96 us per pass: its 16.16 plan
@@ -642,6 +740,82 @@ int fft_plan_radices(int n, int* radix, int* ns)
     return cnt;
 }
 
+bool fft_needs_bluestein(int n)
+{
+    if (n < 2 || n > 512) return false;
+    int rem = n, big = 1;
+    for (int p = 2; p * p <= rem; ++p)
+        while (rem % p == 0) {
+            big = p;
+            rem /= p;
+        }
+    if (rem > 1) big = rem > big ? rem : big;
+    return big > 16;
+}
+
+int fft_bluestein_m(int n)
+{
+    int m = 1;
+    while (m < 2 * n - 1) m <<= 1;
+    return m;
+}
+
+size_t fft_bluestein_elems(int n)
+{
+    const int M = fft_bluestein_m(n);
+    return (size_t)n + 2 * (size_t)M + (size_t)(M / 2);
+}
+
+void fft_bluestein_fill(int n, double2* out)
+{
+    typedef long double ld;
+    const ld pi = 3.14159265358979323846264338327950288L;
+    const int M = fft_bluestein_m(n);
+    int bits = 0;
+    while ((1 << bits) < M) ++bits;
+    // w_e = exp(-pi i e^2 / n), the exponent reduced mod 2n first
+    std::vector<ld> wr(n), wi(n);
+    for (int e = 0; e < n; ++e) {
+        const long long r = ((long long)e * e) % (2ll * n);
+        const ld ang = pi * (ld)r / (ld)n;
+        wr[e] = cosl(ang);
+        wi[e] = -sinl(ang);
+        out[e] = make_double2((double)wr[e], (double)wi[e]);
+    }
+    std::vector<ld> cr(M), ci(M);   // exp(-2 pi i t / M)
+    for (int t = 0; t < M; ++t) {
+        cr[t] = cosl(2 * pi * (ld)t / (ld)M);
+        ci[t] = -sinl(2 * pi * (ld)t / (ld)M);
+    }
+    for (int sg = 0; sg < 2; ++sg) {
+        // kernel h_d = conj(w(sign)_d), w(-1) = w, w(+1) = conj(w): h = conj(w) for sign -1, w for +1;
+        // placed at d and M - d
+        std::vector<ld> hr(M, 0), hi(M, 0);
+        for (int d = 0; d < n; ++d) {
+            const ld re = wr[d], im = sg == 0 ? -wi[d] : wi[d];
+            hr[d] = re;
+            hi[d] = im;
+            if (d > 0) {
+                hr[M - d] = re;
+                hi[M - d] = im;
+            }
+        }
+        for (int k = 0; k < M; ++k) {   // DFT (exp(-2 pi i jk / M)) / M, stored bit-reversed
+            ld sr = 0, si = 0;
+            for (int j = 0; j < M; ++j) {
+                const int t = (int)(((long long)j * k) & (M - 1));
+                sr += hr[j] * cr[t] - hi[j] * ci[t];
+                si += hr[j] * ci[t] + hi[j] * cr[t];
+            }
+            int br = 0;
+            for (int b = 0; b < bits; ++b)
+                if (k & (1 << b)) br |= 1 << (bits - 1 - b);
+            out[n + sg * M + br] = make_double2((double)(sr / M), (double)(si / M));
+        }
+    }
+    for (int t = 0; t < M / 2; ++t) out[n + 2 * M + t] = make_double2((double)cr[t], (double)ci[t]);
+}
+
 int fft_tile_vectors(int n)
 {
     if (const InplacePlan* ip = inplace_plan_for(n)) return ip->kb;
@@ -658,6 +832,17 @@ size_t fft_pass_smem_bytes(const FftPassArgs& a)
 cudaError_t fft_pass_launch(const double2* src, double2* dst, const FftPassArgs& a, int ntiles, int sign,
                             cudaStream_t stream, int nz)
 {
+    if (a.bluestein && fft_needs_bluestein(a.n)) {
+        const int M = fft_bluestein_m(a.n);
+        const size_t sm = (size_t)kBluesteinVec * M * sizeof(double2);
+        dim3 grid((a.nvec + kBluesteinVec - 1) / kBluesteinVec, ntiles, nz);
+        auto goB = [&](auto kern) {
+            if (sm > 48 * 1024) cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+            kern<<<grid, 256, sm, stream>>>(src, dst, a, M);
+        };
+        sign < 0 ? goB(fft_bluestein_kernel<-1>) : goB(fft_bluestein_kernel<1>);
+        return cudaGetLastError();
+    }
     const InplacePlan* ip = inplace_plan_of(a);
     // one butterfly per thread in the widest stage, up to 256 threads (the in-place kernels run
     // 256 threads, each with the butterflies per stage their plan gives)
@@ -716,6 +901,7 @@ void fft_set_fused(int n, int on)
 // passes' tile vectors that divides the layer count; 0 when the passes cannot be fused.
 int fft_fused_chunk(const FftPassArgs& p0, const FftPassArgs& p1)
 {
+    if ((p0.bluestein || p1.bluestein) && fft_needs_bluestein(p0.n)) return 0;   // the Bluestein pass has no fused form
     if (p0.n != p1.n || p0.nvec != p1.nvec || p0.kb != p1.kb || p0.nstages != p1.nstages || p0.nstages == 0) return 0;
     for (int st = 0; st < p0.nstages; ++st)
         if (p0.radix[st] != p1.radix[st]) return 0;

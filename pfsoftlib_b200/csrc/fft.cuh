@@ -29,7 +29,20 @@ struct FftPassArgs {
     const double2* const* srcs;
     double2* const* dsts;
     int coherent;                // first-stage loads through the coherent path (0: read-only path)
+    // lengths with a prime factor above 16 (fft_needs_bluestein): Bluestein's chirp tables
+    // (fft_bluestein_fill); null keeps the direct O(R^2) stages for that factor
+    const double2* bluestein;
 };
+
+// Bluestein's algorithm for a length n <= 512 whose largest prime factor exceeds 16: the DFT as a
+// cyclic convolution of length M (the power of two >= 2n - 1) done with two radix-2 transforms in
+// shared memory (X_k = w_k sum_e x_e w_e conj(w_(k-e)), w_e = exp(sign pi i e^2 / n)).
+bool fft_needs_bluestein(int n);
+int fft_bluestein_m(int n);
+size_t fft_bluestein_elems(int n);   // double2 entries of the table
+// The table, computed on the host in long double: w_e (e < n, sign -1), the bit-reversed length-M
+// transforms of the chirp kernel for sign -1 and +1 (1/M included), exp(-2 pi i t / M) (t < M/2).
+void fft_bluestein_fill(int n, double2* out);
 
 // Radix plan for length n; returns the number of stages (0 if n cannot be planned).
 int fft_plan_radices(int n, int* radix, int* ns);

@@ -101,6 +101,7 @@ FftPassArgs slab_pass(int n, int nvec, const BandTables& t, FftStrides src, FftS
     a.dst = dst;
     a.scale = scale;
     a.twiddle = t.twiddle;
+    a.bluestein = t.bluestein;
     return a;
 }
 

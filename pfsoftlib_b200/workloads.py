@@ -5,6 +5,8 @@ example). ``python -m pfsoftlib_b200.workloads <name> [reps]``:
   batch-<B>x<T>   a batch plan of T transforms at bandwidth B, IDSOFT then DSOFT
   mixed           256 transforms, B uniform over {32,48,64,96,128} (seed 2), batched
   <name>-split    a batch or mixed workload through the split-precision tensor-core DWT
+  <name>-fusedfft any of the above with both FFT passes of a direction in one launch
+                  (pfsoft_tune_fft_fused), restored to the default afterwards
   shard-<B>x<P>   IDSOFT then DSOFT of one transform sharded over P ranks, the ranks run one after
                   another on this GPU (the all-to-all as device copies between their buffers)
   slab-<B>x<P>    the forward and inverse FFT passes of rank 0's layer slab of a P-rank plan
@@ -29,6 +31,12 @@ def run(name: str, reps: int = 1) -> float:
     from . import load
 
     lib = load()
+    if name.endswith("-fusedfft"):
+        assert lib.pfsoft_tune_fft_fused(0, 1) == 0
+        try:
+            return run(name[: -len("-fusedfft")], reps)
+        finally:
+            lib.pfsoft_tune_fft_fused(0, 0)
     s = torch.cuda.current_stream().cuda_stream
     if name.startswith("single-"):
         B = int(name.split("-")[1])

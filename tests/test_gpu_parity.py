@@ -67,9 +67,10 @@ def test_idsoft_matches_reference_golden(lib, golden, B):
     assert orc.max_abs(grid, g["grid"]) <= ABS_TOL
 
 
-@pytest.mark.parametrize("B", [1, 3, 5, 6, 7, 12, 24, 48])
+@pytest.mark.parametrize("B", [1, 3, 5, 6, 7, 12, 17, 24, 37, 48])
 def test_dsoft_matches_oracle_any_grid(lib, oracle, B):
-    # generic (not band-limited) grids, FFT lengths 2, 6, 10, 12, 14, 24, 48, 96
+    # generic (not band-limited) grids, FFT lengths 2, 6, 10, 12, 14, 24, 48, 96; 34 and 74 (prime
+    # factors 17 and 37) run the Bluestein pass
     grid = random_grid(B, seed=100 + B)
     f, _ = gpu_dsoft(lib, grid, B)
     ref = oracle.dsoft(grid)
@@ -77,7 +78,7 @@ def test_dsoft_matches_oracle_any_grid(lib, oracle, B):
     assert orc.max_abs(f, ref) <= ABS_TOL
 
 
-@pytest.mark.parametrize("B", [1, 3, 5, 7, 12, 24, 48])
+@pytest.mark.parametrize("B", [1, 3, 5, 7, 12, 17, 24, 37, 48])
 def test_idsoft_matches_oracle(lib, oracle, B):
     c = orc.coeffs_uniform(B, seed=200 + B)
     grid = gpu_idsoft(lib, c, B)
@@ -86,7 +87,7 @@ def test_idsoft_matches_oracle(lib, oracle, B):
     assert orc.max_abs(grid, ref) <= ABS_TOL * max(1, B)
 
 
-@pytest.mark.parametrize("B", [16, 32, 64, 96, 128, 192])
+@pytest.mark.parametrize("B", [16, 32, 64, 96, 128, 137, 192, 251])
 def test_round_trip_reference_criterion(lib, B):
     c = orc.coeffs_uniform(B, seed=B)
     grid = gpu_idsoft(lib, c, B)
@@ -187,7 +188,7 @@ def test_host_staged_pageable_large_matches_device(lib):
 
 @pytest.mark.parametrize("cols,rows,lays", [(8, 8, 3), (32, 32, 5), (24, 40, 2), (7, 9, 3), (256, 256, 2), (512, 512, 1),
                                              (512, 384, 5), (384, 512, 6), (96, 192, 3), (192, 96, 2),
-                                             (32, 96, 4)])
+                                             (32, 96, 4), (502, 34, 1), (274, 22, 2)])
 def test_layer_wise_fft_matches_numpy(lib, cols, rows, lays):
     rng = np.random.default_rng(cols * rows)
     x = rng.standard_normal((lays, cols, rows)) + 1j * rng.standard_normal((lays, cols, rows))
