@@ -488,12 +488,15 @@ __global__ void __launch_bounds__(256, Tile::kMinBlocks) fft_fused_kernel(const 
     __shared__ int s_item;
     int* ctl = fused_sync(f, 0);
     const int T1 = f.cx[0] * f.ny[0], T2 = f.cx[1] * f.ny[1];
+    if (threadIdx.x == 0) s_item = atomicAdd(ctl, 1);
+    __syncthreads();
     for (;;) {
-        if (threadIdx.x == 0) s_item = atomicAdd(ctl, 1);
-        __syncthreads();
         const int item = s_item;
         __syncthreads();
         if (item >= f.total) break;
+        // the next item is claimed now; thread 0 waits for the counter's answer only after this tile
+        int next = 0;
+        if (threadIdx.x == 0) next = atomicAdd(ctl, 1);
         const int z = item / f.per_z;
         int j = item - z * f.per_z;
         int pass, c, t;
@@ -564,19 +567,23 @@ __global__ void __launch_bounds__(256, Tile::kMinBlocks) fft_fused_kernel(const 
                     asm volatile("discard.global.L2 [%0], 128;" ::"l"(line) : "memory");
             }
         }
+        if (threadIdx.x == 0) s_item = next;
+        __syncthreads();
     }
 }
 
 // Bluestein pass: kBluesteinVec vectors per CTA, each loaded, multiplied by its chirp and
-// zero-padded to M in shared memory, transformed (radix-2, decimation in frequency: natural order
-// in, bit-reversed out), multiplied by the bit-reversed transform of the chirp kernel (1/M
+// zero-padded to M in shared memory, transformed (radix-2 stages, two per pass over shared memory;
+// decimation in frequency: natural order in, bit-reversed out), multiplied by the bit-reversed
+// transform of the chirp kernel (1/M
 // included), transformed back (decimation in time: bit-reversed in, natural out), multiplied by
 // the chirp and stored. The same HBM access pattern as a pass kernel's first and last stages.
 constexpr int kBluesteinVec = 4;
 
 template <int SIGN>
-__global__ void __launch_bounds__(256) fft_bluestein_kernel(const double2* src, double2* dst, const FftPassArgs a, int M)
+__global__ void __launch_bounds__(256) fft_bluestein_kernel(const double2* src, double2* dst, const FftPassArgs a, int logM)
 {
+    const int M = 1 << logM;
     extern __shared__ double2 smem[];   // [kBluesteinVec][M]
     if (a.srcs) {
         src = a.srcs[blockIdx.z];
@@ -598,7 +605,7 @@ __global__ void __launch_bounds__(256) fft_bluestein_kernel(const double2* src, 
             e = t / kBluesteinVec;
         } else {
             e = t & (M - 1);
-            v = t / M;
+            v = t >> logM;
         }
         double2 x = make_double2(0.0, 0.0);
         if (v < nv && e < n) {
@@ -609,27 +616,63 @@ __global__ void __launch_bounds__(256) fft_bluestein_kernel(const double2* src, 
         smem[v * M + e] = x;
     }
     __syncthreads();
-    for (int span = half; span >= 1; span >>= 1) {
-        const int tstep = half / span;
+    // forward, decimation in frequency: two radix-2 stages (spans 2^ls and 2^(ls-1)) per pass over
+    // shared memory, the same arithmetic as one stage at a time
+    int ls = logM - 1;
+    for (; ls >= 1; ls -= 2) {
+        const int sp = 1 << ls, h = sp >> 1, tA = logM - 1 - ls, tB = logM - ls;
+        for (int b = threadIdx.x; b < kBluesteinVec * (M >> 2); b += blockDim.x) {
+            const int i = b & (h - 1);
+            const int p0 = ((b >> (ls - 1)) << (ls + 1)) + i, p1 = p0 + h, p2 = p0 + sp, p3 = p2 + h;
+            const double2 x0 = smem[p0], x1 = smem[p1], x2 = smem[p2], x3 = smem[p3];
+            const double2 a0 = cadd(x0, x2), a2 = cmul(csub(x0, x2), tw[i << tA]);
+            const double2 a1 = cadd(x1, x3), a3 = cmul(csub(x1, x3), tw[(i + h) << tA]);
+            const double2 wb = tw[i << tB];
+            smem[p0] = cadd(a0, a1);
+            smem[p1] = cmul(csub(a0, a1), wb);
+            smem[p2] = cadd(a2, a3);
+            smem[p3] = cmul(csub(a2, a3), wb);
+        }
+        __syncthreads();
+    }
+    if (ls == 0) {   // an odd number of stages: the last one alone (span 1, twiddle 1)
         for (int b = threadIdx.x; b < kBluesteinVec * half; b += blockDim.x) {
-            const int v = b / half, i2 = b - v * half;
-            const int blk = i2 / span, i = i2 - blk * span;
-            const int p = v * M + blk * 2 * span + i, q = p + span;
-            const double2 u = smem[p], x = smem[q];
+            const int p = b << 1;
+            const double2 u = smem[p], x = smem[p + 1];
             smem[p] = cadd(u, x);
-            smem[q] = cmul(csub(u, x), tw[i * tstep]);
+            smem[p + 1] = csub(u, x);
         }
         __syncthreads();
     }
     for (int t = threadIdx.x; t < kBluesteinVec * M; t += blockDim.x) smem[t] = cmul(smem[t], fh[t & (M - 1)]);
     __syncthreads();
-    for (int span = 1; span <= half; span <<= 1) {
-        const int tstep = half / span;
+    // inverse, decimation in time: spans 2^ls and 2^(ls+1) per pass (conjugate twiddles)
+    ls = 0;
+    for (; ls + 1 < logM; ls += 2) {
+        const int sp = 1 << ls, t1 = logM - 1 - ls, t2 = logM - 2 - ls;
+        for (int b = threadIdx.x; b < kBluesteinVec * (M >> 2); b += blockDim.x) {
+            const int i = b & (sp - 1);
+            const int p0 = ((b >> ls) << (ls + 2)) + i, p1 = p0 + sp, p2 = p1 + sp, p3 = p2 + sp;
+            double2 w = tw[i << t1];
+            w.y = -w.y;
+            const double2 x0 = smem[p0], x1 = cmul(smem[p1], w), x2 = smem[p2], x3 = cmul(smem[p3], w);
+            const double2 a0 = cadd(x0, x1), a1 = csub(x0, x1), a2 = cadd(x2, x3), a3 = csub(x2, x3);
+            double2 w0 = tw[i << t2], w1 = tw[(i + sp) << t2];
+            w0.y = -w0.y;
+            w1.y = -w1.y;
+            const double2 b2 = cmul(a2, w0), b3 = cmul(a3, w1);
+            smem[p0] = cadd(a0, b2);
+            smem[p2] = csub(a0, b2);
+            smem[p1] = cadd(a1, b3);
+            smem[p3] = csub(a1, b3);
+        }
+        __syncthreads();
+    }
+    if (ls == logM - 1) {   // the last stage alone (span M/2)
         for (int b = threadIdx.x; b < kBluesteinVec * half; b += blockDim.x) {
-            const int v = b / half, i2 = b - v * half;
-            const int blk = i2 / span, i = i2 - blk * span;
-            const int p = v * M + blk * 2 * span + i, q = p + span;
-            double2 w = tw[i * tstep];
+            const int i = b & (half - 1);
+            const int p = ((b >> (logM - 1)) << logM) + i, q = p + half;
+            double2 w = tw[i];
             w.y = -w.y;
             const double2 u = smem[p], x = cmul(smem[q], w);
             smem[p] = cadd(u, x);
@@ -834,11 +877,13 @@ cudaError_t fft_pass_launch(const double2* src, double2* dst, const FftPassArgs&
 {
     if (a.bluestein && fft_needs_bluestein(a.n)) {
         const int M = fft_bluestein_m(a.n);
+        int logM = 0;
+        while ((1 << logM) < M) ++logM;
         const size_t sm = (size_t)kBluesteinVec * M * sizeof(double2);
         dim3 grid((a.nvec + kBluesteinVec - 1) / kBluesteinVec, ntiles, nz);
         auto goB = [&](auto kern) {
             if (sm > 48 * 1024) cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-            kern<<<grid, 256, sm, stream>>>(src, dst, a, M);
+            kern<<<grid, 256, sm, stream>>>(src, dst, a, logM);
         };
         sign < 0 ? goB(fft_bluestein_kernel<-1>) : goB(fft_bluestein_kernel<1>);
         return cudaGetLastError();
