@@ -911,9 +911,9 @@ def main():
     d = stages[dominant]
     # DRAM bytes per launch (read + write) of these kernels at B = 128, from one ncu capture of the
     # same launches (dram__bytes_read.sum + dram__bytes_write.sum)
-    traffic = {"dwt_forward": 268.37e6 + 43.51e6, "dwt_inverse": 46.44e6 + 208.20e6,
-               "fft_forward_gamma": 268.5e6 + 221.6e6, "fft_inverse_alpha": 268.5e6 + 214.7e6,
-               "fft_inverse_gamma": 268.5e6 + 219.7e6}
+    traffic = {"dwt_forward": 277.00e6 + 39.89e6, "dwt_inverse": 55.02e6 + 206.65e6,
+               "fft_forward_gamma": 268.51e6 + 217.40e6, "fft_forward_alpha": 268.50e6 + 206.99e6,
+               "fft_inverse_alpha": 268.51e6 + 206.85e6, "fft_inverse_gamma": 268.51e6 + 217.70e6}
     roofline = {"kernel": dominant, "bound": d["bound"], "achieved": d["achieved"], "peak": d["peak"],
                 "unit": d["unit"], "frac": d["frac"], "traffic": traffic.get(dominant),
                 "peak_source": ("measured FP64 MMA peak (own micro-benchmark; MEASURED_PEAKS.json has no FP64 entry)"
