@@ -122,7 +122,8 @@ constexpr int kOffCoef = kOffRaw + kRaw * kRawBytes;   // generators: 32 steps x
 constexpr int kOffEpi = kOffCoef + kGenWarps * 32 * 4 * 8;   // epilogue: 16 x {1/scale re, im} per warp
 constexpr int kSegCache = 256;                      // segment starts kept in shared memory
 constexpr int kOffSeg = kOffEpi + 4 * 16 * 16;     // first item of each segment (the first kSegCache)
-constexpr int kOffBar = kOffSeg + kSegCache * 4;
+constexpr int kOffCase = kOffSeg + kSegCache * 4;   // epilogue: the item's 8 cases, 32 B each, per warp
+constexpr int kOffBar = kOffCase + 4 * 8 * 32;
 // mbarriers: full[kStages], empty[kStages], accfull[2], accempty[2], rawfull[kRaw], drain, never
 // (test knob)
 constexpr int kBarFull = 0, kBarEmpty = kStages, kBarAccFull = 2 * kStages, kBarAccEmpty = 2 * kStages + kAccSets,
@@ -210,6 +211,15 @@ __device__ __forceinline__ void column_scale(double m, double& cs47, double& ics
     cs47 = ldexp(1.0, 46 - e);   // 2^-(e+1) * 2^47
     ics = ldexp(1.0, e + 1);
 }
+
+// One case of an item as the epilogue stores it: bin offset (row N + col) N, orders, beta
+// reversal and sign factor (class_case).
+struct CaseEnt {
+    long long off;
+    int m1, m2, rev, pad;
+    double s0;
+};
+static_assert(sizeof(CaseEnt) == 32, "case entry size");
 
 // Item geometry shared by every role.
 struct ItemGeo {
@@ -589,6 +599,7 @@ __global__ void __launch_bounds__(kThreads, 1)
         const int q4 = warp & 3;   // tensor-memory lane quarter
         const int row = 32 * q4 + lane;
         double2* s_ics = reinterpret_cast<double2*>(smem + kOffEpi) + 16 * q4;
+        CaseEnt* s_ce = reinterpret_cast<CaseEnt*>(smem + kOffCase) + 8 * q4;
         auto next_item = [&](int& r) -> int {
             for (;; ++r) {
                 const int idx = cta_item(r, n_items);
@@ -630,14 +641,29 @@ __global__ void __launch_bounds__(kThreads, 1)
             tc::fence_after_sync();
             __syncwarp();
             if (lane < 16) s_ics[lane] = ics_c;
-            __syncwarp();
             const int N = it.N, B = it.B;
+            if (lane < it.nc) {   // the item's cases, once per item instead of per lane and value
+                const PairCase p = class_case(it.M, it.Mp, lane, N);
+                CaseEnt ce;
+                ce.off = ((long long)p.row * N + p.col) * N;
+                ce.m1 = p.m1;
+                ce.m2 = p.m2;
+                ce.rev = p.rev;
+                ce.pad = 0;
+                ce.s0 = p.s0;
+                s_ce[lane] = ce;
+            }
+            __syncwarp();
             const uint32_t taddr = tmem + ((uint32_t)(32 * q4) << 16) + (uint32_t)(a * kAccStride);
             // forward: degree l of this lane; inverse: beta k
             const int l = it.M + 128 * it.tile + row;
             const int k = 128 * it.tile + row;
             const bool live = DIR == 0 ? (l < B) : (k < N);
+            const int Ll = 2 * l + 1;
+            const long long coff = DIR == 0 ? (long long)coef_offset(l) : 0;
+            const double fnorm = DIR == 0 ? (kPi / (double)(B * 2 * B)) * rowf_c : 0.0;   // src/fn_dsoft.cpp:119
             for (int t = 0; t < it.nt; ++t) {
+                double2* const outp = DIR == 0 ? it.gr->coeffs[it.t0 + t] : it.gr->X[it.t0 + t];
                 int32_t acc[kPlanes][16];
 #pragma unroll
                 for (int e = 0; e < kPlanes; ++e) tc::tmem_ld16(taddr + (uint32_t)(16 * it.nt * e + 16 * t), acc[e]);
@@ -654,15 +680,15 @@ __global__ void __launch_bounds__(kThreads, 1)
 #pragma unroll
                 for (int q = 0; q < 8; ++q) {
                     if (q >= it.nc) break;
-                    const PairCase p = class_case(it.M, it.Mp, q, N);
+                    const CaseEnt ce = s_ce[q];
                     const double2 ics = s_ics[8 * t + q];
                     if (DIR == 0) {
-                        const double f = (kPi / (double)(B * 2 * B)) * rowf_c * case_sign(p, l, it.M);   // src/fn_dsoft.cpp:119
-                        it.gr->coeffs[it.t0 + t][coef_index(l, p.m1, p.m2)] =
-                            make_double2(f * v[2 * q] * ics.x, f * v[2 * q + 1] * ics.y);
+                        // coef_index(l, m1, m2) and case_sign of class_case(M, M', q)
+                        const int i1 = ce.m1 >= 0 ? ce.m1 : Ll + ce.m1, i2 = ce.m2 >= 0 ? ce.m2 : Ll + ce.m2;
+                        const double f = fnorm * ((ce.rev && ((l - it.M) & 1)) ? -ce.s0 : ce.s0);
+                        outp[coff + (long long)i2 * Ll + i1] = make_double2(f * v[2 * q] * ics.x, f * v[2 * q + 1] * ics.y);
                     } else {
-                        it.gr->X[it.t0 + t][((size_t)p.row * N + p.col) * N + (p.rev ? N - 1 - k : k)] =
-                            make_double2(v[2 * q] * ics.x, v[2 * q + 1] * ics.y);
+                        outp[ce.off + (ce.rev ? N - 1 - k : k)] = make_double2(v[2 * q] * ics.x, v[2 * q + 1] * ics.y);
                     }
                 }
             }
