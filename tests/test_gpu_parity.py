@@ -188,7 +188,7 @@ def test_host_staged_pageable_large_matches_device(lib):
 
 @pytest.mark.parametrize("cols,rows,lays", [(8, 8, 3), (32, 32, 5), (24, 40, 2), (7, 9, 3), (256, 256, 2), (512, 512, 1),
                                              (512, 384, 5), (384, 512, 6), (96, 192, 3), (192, 96, 2),
-                                             (32, 96, 4), (502, 34, 1), (274, 22, 2)])
+                                             (32, 96, 4), (502, 34, 1), (274, 22, 2), (257, 6, 2), (6, 257, 2)])
 def test_layer_wise_fft_matches_numpy(lib, cols, rows, lays):
     rng = np.random.default_rng(cols * rows)
     x = rng.standard_normal((lays, cols, rows)) + 1j * rng.standard_normal((lays, cols, rows))
