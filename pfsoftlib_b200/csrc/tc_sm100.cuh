@@ -117,7 +117,7 @@ __device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t* mbar, uint32_t b
                  : "memory");
 }
 
-// ---- bulk copy global -> shared (untiled, no multicast), completion on an mbarrier ------------
+// ---- bulk copy global -> this CTA's shared memory (untiled), completion on an mbarrier --------
 // Both addresses 16-byte aligned, `bytes` a multiple of 16; the destination is this CTA's own
 // shared memory.
 __device__ __forceinline__ void bulk_g2s(void* dst_smem, const void* src_gmem, uint32_t bytes, uint64_t* mbar)
