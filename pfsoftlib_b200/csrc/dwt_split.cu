@@ -35,19 +35,19 @@
 // class's degrees over the whole array). Each copy also brings the columns' scale entries.
 // One CTA of 12 warps per SM, roles fixed per warp:
 //   warp 0      issues the MMAs (one lane) into one of two accumulator sets in tensor memory;
-//   warp 1      issues the bulk copies of each chunk's data into a ring of raw slots;
-//   warps 2-3   digitise a chunk's raw data (alternate chunks) into the stage's B operand;
+//   warps 1-3   loaders: chunk g to warp 1 + g % 3, which issues the chunk's bulk copies two of its
+//               chunks ahead into one of its two raw slots, then digitises the raw data into the
+//               stage's B operand;
 //   warps 4-7   epilogue: read an accumulator set back (warp w reads lanes 32(w%4) ..), combine, store;
 //   warps 8-11  generators: the Wigner rows of a chunk to digit planes (forward: one warp per
 //               chunk of 32 beta columns, all rows; inverse: the four warps on the tile's 128 beta
 //               columns, 32 degrees per chunk).
 // Chunks move through a ring of shared-memory stages (full / empty mbarriers; empty is signalled by
-// tcgen05.commit) and raw slots (rawfull by the copies' byte count, rawempty by the digitising
-// warp), accumulator sets through accfull / accempty, so copies, generation, digitisation, MMAs and
-// the epilogue of different chunks and items overlap. Every wait is bounded (%globaltimer); a wait
-// that runs out sets a CTA-wide abort flag, every role leaves, the copy warp waits (bounded) for
-// its copies in flight and the MMA lane for its committed MMAs before the CTA ends, and *status is
-// set to 1.
+// tcgen05.commit) and the loaders' raw slots (rawfull by the copies' byte count), accumulator sets
+// through accfull / accempty, so copies, generation, digitisation, MMAs and the epilogue of
+// different chunks and items overlap. Every wait is bounded (%globaltimer); a wait that runs out
+// sets a CTA-wide abort flag, every role leaves, each loader waits (bounded) for its copies in
+// flight and the MMA lane for its committed MMAs before the CTA ends, and *status is set to 1.
 //
 // Operand layouts in shared memory (no swizzle; see tc_sm100.cuh), per stage and plane:
 //   A forward (MN-major, rows = degrees):  (r/16)*512 + (k/8)*128 + (k%8)*16 + (r%16)
