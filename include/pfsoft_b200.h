@@ -197,10 +197,10 @@ int pfsoft_server_create(size_t budget_bytes, int max_batch, int streams, pfsoft
  * direction and ANY bandwidths (1 <= B <= 256; larger ones are rejected with PFSOFT_EINVAL) and runs
  * their discrete Wigner transforms in one split-precision launch (the arithmetic of
  * PFSOFT_BATCH_SPLIT; FFT passes per bandwidth). A request's workspace then also holds the split
- * kernel's operand area: pfsoft_workspace_bytes(B) plus (8B(B+1) + B + 280 C(B)) * 16 bytes,
- * C(B) = sum over m < B of (m+1) ceil((B-m)/32) (the inverse's class-major operand; about a
- * quarter of the grid bytes at B = 128 and 256). A bounded wait that ran out finishes that
- * batch's requests with PFSOFT_ETIMEOUT. */
+ * kernel's operand area: pfsoft_workspace_bytes(B) plus (8B(B+1) + B) * 16 + 6144 ceil(D(B)/2)
+ * bytes, D(B) = B(B+1)/2 ceil(B/16) (the data operand's digit blocks, one per class and 32-sample
+ * chunk; about three quarters of the grid bytes at B = 128 and 256). A bounded wait that ran out
+ * finishes that batch's requests with PFSOFT_ETIMEOUT. */
 #define PFSOFT_SERVER_SPLIT 1
 int pfsoft_server_create_ex(size_t budget_bytes, int max_batch, int streams, int flags, pfsoft_server** out);
 int pfsoft_server_destroy(pfsoft_server* srv);

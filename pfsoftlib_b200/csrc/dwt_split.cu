@@ -28,26 +28,24 @@
 // dwt_split_segments, largest bandwidth first), and item i of a segment is class i / (pairs *
 // tiles) -- classes run longest first (M ascending) -- then transform pair, then tile.
 //
-// The data operand reaches shared memory by untiled bulk copies (cp.async.bulk, completion on an
-// mbarrier), never by per-thread gathers: forward, the chunk's 32 beta of each case's bin column
-// (contiguous in the spectrum); inverse, a class-major copy of the scaled coefficients that
-// split_inv_prepare_kernel writes once per launch (the packed coefficient layout scatters a
-// class's degrees over the whole array). Each copy also brings the columns' scale entries.
+// The data operand is digitised before the launch: split_fwd_prepare_kernel (the spectrum's bin
+// columns over beta) and split_inv_prepare_kernel (the scaled coefficients, degrees of a class
+// gathered from the packed layout) write each column's scale entries and its digit planes, one
+// block per chunk already in the B operand's shared-memory layout, so that a chunk reaches its
+// stage as one untiled bulk copy (cp.async.bulk, completion on an mbarrier by the byte count).
 // One CTA of 12 warps per SM, roles fixed per warp:
 //   warp 0      issues the MMAs (one lane) into one of two accumulator sets in tensor memory;
-//   warps 1-3   loaders: chunk g to warp 1 + g % 3, which issues the chunk's bulk copies two of its
-//               chunks ahead into one of its two raw slots, then digitises the raw data into the
-//               stage's B operand;
+//   warp 1      issues each chunk's bulk copy as soon as its stage is empty;
 //   warps 4-7   epilogue: read an accumulator set back (warp w reads lanes 32(w%4) ..), combine, store;
 //   warps 8-11  generators: the Wigner rows of a chunk to digit planes (forward: one warp per
-//               chunk of 32 beta columns, all rows; inverse: the four warps on the tile's 128 beta
-//               columns, 32 degrees per chunk).
-// Chunks move through a ring of shared-memory stages (full / empty mbarriers; empty is signalled by
-// tcgen05.commit) and the loaders' raw slots (rawfull by the copies' byte count), accumulator sets
-// through accfull / accempty, so copies, generation, digitisation, MMAs and the epilogue of
-// different chunks and items overlap. Every wait is bounded (%globaltimer); a wait that runs out
-// sets a CTA-wide abort flag, every role leaves, each loader waits (bounded) for its copies in
-// flight and the MMA lane for its committed MMAs before the CTA ends, and *status is set to 1.
+//               chunk of 32 beta columns, all rows, with warps 2-3 as two more; inverse: the four
+//               warps on the tile's 128 beta columns, 32 degrees per chunk; warps 2-3 idle).
+// Chunks move through a ring of shared-memory stages (full by the generators, copy by the bytes,
+// empty by tcgen05.commit), accumulator sets through accfull / accempty, so copies, generation,
+// MMAs and the epilogue of different chunks and items overlap. Every wait is bounded
+// (%globaltimer); a wait that runs out sets a CTA-wide abort flag, every role leaves, the copy
+// warp waits (bounded) for its copies in flight and the MMA lane for its committed MMAs before the
+// CTA ends, and *status is set to 1.
 //
 // Operand layouts in shared memory (no swizzle; see tc_sm100.cuh), per stage and plane:
 //   A forward (MN-major, rows = degrees):  (r/16)*512 + (k/8)*128 + (k%8)*16 + (r%16)
@@ -92,17 +90,15 @@ using namespace dwtk;
 constexpr int kNT = 2;                 // transforms per work item (at most)
 constexpr int kPlanes = 6;             // digits per operand
 constexpr int kKC = 32;                // K per chunk: one kind::i8 MMA
-constexpr int kStages = 5;             // operand ring
-constexpr int kLoadWarps = 3;          // loader warps (bulk copies + digitising)
-constexpr int kRawPerWarp = 2;         // raw slots per loader warp
-constexpr int kRaw = kLoadWarps * kRawPerWarp;
+constexpr int kStages = 7;             // operand ring
 constexpr int kAccSets = 2;
 constexpr int kAccStride = 256;        // tensor-memory columns between the two accumulator sets
 constexpr uint32_t kTmemCols = 512;
 constexpr int kThreads = 384;
-constexpr int kLoadWarp0 = 1;
+constexpr int kLoadWarp = 1;           // bulk copies of the data operand
 constexpr int kEpiWarp0 = 4;
-constexpr int kGenWarp0 = 8, kGenWarps = 4;
+// generators: warps 8-11 in both directions; forward also warps 2-3 (one warp per chunk)
+constexpr int kGenWarp0 = 8, kGenWarpsInv = 4, kGenWarpsFwd = 6;
 constexpr uint64_t kWaitNs = 2000000000ull;   // 2 s
 
 constexpr int kAPlane = 4096;                       // 128 rows x 32 bytes of K
@@ -110,30 +106,23 @@ constexpr int kABytes = kPlanes * kAPlane;          // 24 KB
 constexpr int kBRows = 16 * kNT * kPlanes;          // 192
 constexpr int kBBytes = kBRows / 8 * 256;           // 6 KB
 constexpr int kStageBytes = kABytes + kBBytes;
-// raw slot, per transform: 8 scale entries {cs47 re, im}, {1/scale re, im} (256 B), then the 8
-// cases' 32 double2 each at a 528-byte pitch (a quarter warp reading one value of each case hits
-// eight distinct bank groups)
-constexpr int kRawHdr = 256;
-constexpr int kRawPitch = 528;
-constexpr int kRawT = kRawHdr + 8 * kRawPitch;      // 4480
-constexpr int kRawBytes = kNT * kRawT;
-constexpr int kOffRaw = kStages * kStageBytes;
-constexpr int kOffCoef = kOffRaw + kRaw * kRawBytes;   // generators: 32 steps x {c1, f1 f2, f1, row scale} per warp
-constexpr int kOffEpi = kOffCoef + kGenWarps * 32 * 4 * 8;   // epilogue: 16 x {1/scale re, im} per warp
-constexpr int kSegCache = 256;                      // segment starts kept in shared memory
-constexpr int kOffSeg = kOffEpi + 4 * 16 * 16;     // first item of each segment (the first kSegCache)
-constexpr int kOffCase = kOffSeg + kSegCache * 4;   // epilogue: the item's 8 cases, 32 B each, per warp
+// data-operand digits of one chunk and transform: 6 planes x 16 rows x 32 K (the B layout)
+constexpr int kDigT = kPlanes * 512;                // 3072
+constexpr int kDigPair = kNT * kDigT;               // 6144: a transform pair's block
+constexpr int kOffCoef = kStages * kStageBytes;     // generators: 32 steps x {c1, f1 f2, f1, row scale} per warp
+constexpr int kOffEpi = kOffCoef + kGenWarpsFwd * 32 * 4 * 8;   // epilogue: 16 x {1/scale re, im} per warp
+constexpr int kSegCache = 192;                      // segments kept in shared memory (32 B each)
+constexpr int kOffSeg = kOffEpi + 4 * 16 * 16;     // the first kSegCache segments of the launch
+constexpr int kOffCase = kOffSeg + kSegCache * 32;  // epilogue: the item's 8 cases, 32 B each, per warp
 constexpr int kOffBar = kOffCase + 4 * 8 * 32;
-// mbarriers: full[kStages], empty[kStages], accfull[2], accempty[2], rawfull[kRaw], drain, never
-// (test knob)
-constexpr int kBarFull = 0, kBarEmpty = kStages, kBarAccFull = 2 * kStages, kBarAccEmpty = 2 * kStages + kAccSets,
-              kBarRawFull = 2 * kStages + 2 * kAccSets, kBarDrain = kBarRawFull + kRaw, kBarNever = kBarDrain + 1,
+// mbarriers: full[kStages] (generators), copy[kStages] (the data operand's bytes), empty[kStages],
+// accfull[2], accempty[2], drain, never (test knob)
+constexpr int kBarFull = 0, kBarCopy = kStages, kBarEmpty = 2 * kStages, kBarAccFull = 3 * kStages,
+              kBarAccEmpty = 3 * kStages + kAccSets, kBarDrain = 3 * kStages + 2 * kAccSets, kBarNever = kBarDrain + 1,
               kNumBars = kBarNever + 1;
 constexpr int kOffMisc = kOffBar + kNumBars * 8;    // tensor-memory address, abort flag
 constexpr int kSmemBytes = kOffMisc + 16;
-static_assert(kStageBytes % 1024 == 0, "stages stay 1 KB aligned");
-static_assert(kRawT % 16 == 0 && kRawPitch % 16 == 0 && kOffRaw % 16 == 0, "bulk-copy destinations 16-byte aligned");
-constexpr int kInvChunk = kRawT / 16;               // double2 per inverse chunk block (280)
+static_assert(kStageBytes % 1024 == 0 && kABytes % 16 == 0, "stages stay 1 KB aligned, B operands 16 B");
 static_assert(kSmemBytes <= 227 * 1024, "shared memory");
 static_assert(16 * kNT * kPlanes <= kAccStride, "an accumulator set fits its column range");
 
@@ -147,14 +136,34 @@ constexpr double kMagic = 4503599627370496.0 + 141289400074368.0;
 struct SplitSeg {
     int group, first, count, pairs, tiles, T, B, N;
 };
+static_assert(sizeof(SplitSeg) == 32, "segment cache entries");
 
 // Operand area past each transform's spectrum (double2 offsets from X + N^3): the column scale
-// table (two double2 per (class, case)), the row table (one per degree), the inverse operand in
-// class-major order, one block per 32-degree chunk laid out as a raw slot: the class's 8 scale
-// entries, then 8 cases x 32 degrees at the slot's pitch (kInvChunk double2), so that a chunk of
-// one transform is a single bulk copy.
+// table (two double2 per (class, case)), the row table (one per degree), then the data operand as
+// digit blocks, one per chunk, already in the shared-memory layout of the MMA's B operand.
+// Chunk j of a class-major list (forward: j = class * ceil(N / 32) + beta chunk; inverse:
+// j = inv_chunk_prefix(B, M, M') + degree chunk). A transform pair (t0, t0 + 1) keeps one 6144-byte
+// block per chunk, plane p of transform t0 + h at 512 (2p + h), stored in the area of transform
+// t0 + (j & 1) at (j >> 1) * 6144; an unpaired last transform keeps 3072-byte blocks (plane p at
+// 512 p) in its own area at j * 3072. A chunk of an item is then a single bulk copy.
 __host__ __device__ __forceinline__ size_t aux_rows(int B) { return (size_t)16 * num_classes(B); }
-__host__ __device__ __forceinline__ size_t aux_inv(int B) { return aux_rows(B) + (size_t)B; }
+__host__ __device__ __forceinline__ size_t aux_dig(int B) { return aux_rows(B) + (size_t)B; }
+__host__ __device__ __forceinline__ int fwd_chunks(int N) { return (N + 31) / 32; }
+__host__ __device__ __forceinline__ long long dig_chunks(int B)
+{
+    const long long f = (long long)num_classes(B) * fwd_chunks(2 * B), i = inv_chunk_prefix(B, B, 0);
+    return f > i ? f : i;
+}
+// Byte offset of chunk j's block in the area of transform t0 + (j & 1) (pairs) or t0 (nt = 1),
+// and that transform.
+__host__ __device__ __forceinline__ long long dig_block_off(int nt, long long j)
+{
+    return nt == 2 ? (j >> 1) * kDigPair : j * kDigT;
+}
+__host__ __device__ __forceinline__ int dig_block_owner(int t0, int nt, long long j)
+{
+    return nt == 2 ? t0 + (int)(j & 1) : t0;
+}
 
 // Digit words of four magic-biased values: w[p] holds byte (5 - p) of each value (value i in
 // byte i), XOR 0x80, i.e. plane p of the signed digits, most significant plane first.
@@ -188,16 +197,6 @@ __device__ __forceinline__ void store_unit16(unsigned char* base, int plane_stri
         *reinterpret_cast<uint4*>(base + p * plane_stride) = make_uint4(w0[p], w1[p], w2[p], w3[p]);
 }
 
-// 8 magic-biased values -> one 8-byte half unit per plane
-__device__ __forceinline__ void store_unit8(unsigned char* base, int plane_stride, const double (&z)[8])
-{
-    uint32_t w0[kPlanes], w1[kPlanes];
-    pack4(z[0], z[1], z[2], z[3], w0);
-    pack4(z[4], z[5], z[6], z[7], w1);
-#pragma unroll
-    for (int p = 0; p < kPlanes; ++p) *reinterpret_cast<uint2*>(base + p * plane_stride) = make_uint2(w0[p], w1[p]);
-}
-
 // scale * 2^47 for a column whose largest magnitude is m (|v * scale| < 0.5), and 1 / scale
 __device__ __forceinline__ void column_scale(double m, double& cs47, double& ics)
 {
@@ -227,9 +226,9 @@ struct ItemGeo {
     int B, N, M, Mp, R, nc, t0, nt, tile, cls, nchunks;
 };
 
-__device__ __forceinline__ int seg_first(const SplitSeg* __restrict__ segs, const int* s_first, int j)
+__device__ __forceinline__ int seg_first(const SplitSeg* __restrict__ segs, const SplitSeg* s_seg, int j)
 {
-    return j < kSegCache ? s_first[j] : segs[j].first;
+    return j < kSegCache ? s_seg[j].first : segs[j].first;
 }
 
 // Geometry of item i: its segment by a forward scan from the caller's hint (a role visits items
@@ -238,13 +237,13 @@ __device__ __forceinline__ int seg_first(const SplitSeg* __restrict__ segs, cons
 // role skips it alike).
 template <int DIR>
 __device__ __forceinline__ ItemGeo item_geo(const DwtGroup* __restrict__ groups, const SplitSeg* __restrict__ segs,
-                                            const int* s_first, int nseg, int i, int& hint)
+                                            const SplitSeg* s_seg, int nseg, int i, int& hint)
 {
     int sidx = hint;
-    if (i < seg_first(segs, s_first, sidx)) sidx = 0;
-    while (sidx + 1 < nseg && i >= seg_first(segs, s_first, sidx + 1)) ++sidx;
+    if (i < seg_first(segs, s_seg, sidx)) sidx = 0;
+    while (sidx + 1 < nseg && i >= seg_first(segs, s_seg, sidx + 1)) ++sidx;
     hint = sidx;
-    const SplitSeg sg = segs[sidx];
+    const SplitSeg sg = sidx < kSegCache ? s_seg[sidx] : segs[sidx];
     const int j = i - sg.first;
     const int per_cls = sg.pairs * sg.tiles;
     const int cls = j / per_cls, rem = j - cls * per_cls;
@@ -284,14 +283,14 @@ struct Loc {
 // The first chunk at or after chunk c of the CTA's r-th item (items without chunks skipped).
 template <int DIR>
 __device__ __forceinline__ void locate(Loc& L, int r, int c, const DwtGroup* __restrict__ groups,
-                                       const SplitSeg* __restrict__ segs, const int* s_first, int nseg, int n_items, int& hint)
+                                       const SplitSeg* __restrict__ segs, const SplitSeg* s_seg, int nseg, int n_items, int& hint)
 {
     for (;;) {
         L.idx = cta_item(r, n_items);
         L.r = r;
         L.c = 0;
         if (L.idx < 0) return;
-        L.it = item_geo<DIR>(groups, segs, s_first, nseg, L.idx, hint);
+        L.it = item_geo<DIR>(groups, segs, s_seg, nseg, L.idx, hint);
         if (c < L.it.nchunks) {
             L.c = c;
             return;
@@ -384,6 +383,20 @@ __device__ __forceinline__ void adv16(double& dcur, double& dprev, double cb, co
     }
 }
 
+// L moved on by dc >= 0 chunks of the ring: within its item without recomputing the geometry.
+template <int DIR>
+__device__ __forceinline__ void advance(Loc& L, int dc, const DwtGroup* __restrict__ groups,
+                                        const SplitSeg* __restrict__ segs, const SplitSeg* s_seg, int nseg, int n_items,
+                                        int& hint)
+{
+    if (L.idx < 0) return;
+    if (L.c + dc < L.it.nchunks) {
+        L.c += dc;
+        return;
+    }
+    locate<DIR>(L, L.r + 1, L.c + dc - L.it.nchunks, groups, segs, s_seg, nseg, n_items, hint);
+}
+
 template <int DIR>
 __global__ void __launch_bounds__(kThreads, 1)
     dwt_split_kernel(const DwtGroup* __restrict__ groups, const SplitSeg* __restrict__ segs, int nseg, int n_items,
@@ -394,8 +407,8 @@ __global__ void __launch_bounds__(kThreads, 1)
     uint32_t* s_taddr = reinterpret_cast<uint32_t*>(smem + kOffMisc);
     volatile int* s_abort = reinterpret_cast<volatile int*>(smem + kOffMisc + 4);
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    int* s_first = reinterpret_cast<int*>(smem + kOffSeg);
-    for (int j = tid; j < min(nseg, kSegCache); j += kThreads) s_first[j] = segs[j].first;
+    SplitSeg* s_seg = reinterpret_cast<SplitSeg*>(smem + kOffSeg);
+    for (int j = tid; j < min(nseg, kSegCache); j += kThreads) s_seg[j] = segs[j];
     int hint = 0;   // this warp's segment cursor (items are visited in increasing order)
 
     if (warp == 0) {
@@ -404,14 +417,14 @@ __global__ void __launch_bounds__(kThreads, 1)
     }
     if (tid == 32) {
         for (int s = 0; s < kStages; ++s) {
-            tc::mbar_init(&bars[kBarFull + s], DIR == 0 ? 2 : 1 + kGenWarps);   // generator warp(s) + digitising warp
+            tc::mbar_init(&bars[kBarFull + s], DIR == 0 ? 1 : kGenWarpsInv);   // the chunk's generator warp(s)
+            tc::mbar_init(&bars[kBarCopy + s], 1);                            // arrive.expect_tx + the bytes
             tc::mbar_init(&bars[kBarEmpty + s], 1);                           // tcgen05.commit
         }
         for (int a = 0; a < kAccSets; ++a) {
             tc::mbar_init(&bars[kBarAccFull + a], 1);
             tc::mbar_init(&bars[kBarAccEmpty + a], 4);   // the four epilogue warps
         }
-        for (int r = 0; r < kRaw; ++r) tc::mbar_init(&bars[kBarRawFull + r], 1);   // arrive.expect_tx + the bytes
         tc::mbar_init(&bars[kBarDrain], 1);
         tc::mbar_init(&bars[kBarNever], 1);
         tc::mbar_fence_init();
@@ -431,7 +444,7 @@ __global__ void __launch_bounds__(kThreads, 1)
         for (int r = 0; ok; ++r) {
             const int idx = cta_item(r, n_items);
             if (idx < 0) break;
-            const ItemGeo it = item_geo<DIR>(groups, segs, s_first, nseg, idx, hint);
+            const ItemGeo it = item_geo<DIR>(groups, segs, s_seg, nseg, idx, hint);
             if (it.nchunks == 0) continue;
             const int a = n & 1, ua = n >> 1;
             ++n;
@@ -443,7 +456,8 @@ __global__ void __launch_bounds__(kThreads, 1)
             const uint32_t dbase = tmem + (uint32_t)(a * kAccStride);
             for (int c = 0; c < it.nchunks; ++c, ++g) {
                 const int s = g % kStages, u = g / kStages;
-                if (!tc::mbar_wait_bounded(&bars[kBarFull + s], (uint32_t)(u & 1), kWaitNs, s_abort)) {
+                if (!tc::mbar_wait_bounded(&bars[kBarFull + s], (uint32_t)(u & 1), kWaitNs, s_abort) ||
+                    !tc::mbar_wait_bounded(&bars[kBarCopy + s], (uint32_t)(u & 1), kWaitNs, s_abort)) {
                     ok = false;
                     break;
                 }
@@ -474,123 +488,40 @@ __global__ void __launch_bounds__(kThreads, 1)
                 if (tc::globaltimer_ns() - t0 > kWaitNs) break;
         }
         __syncwarp();
-    } else if (warp >= kLoadWarp0 && warp < kLoadWarp0 + kLoadWarps) {
-        // ------------------------------------------------------------------ loaders (data operand)
-        // Warp L takes chunks g = L + 3j of the ring; its two raw slots alternate (chunk j in slot
-        // 2L + j%2). The bulk copies of chunk j+2 are issued as soon as chunk j has been digitised,
-        // so two chunks of copies per warp are in flight (several issuing warps: one warp issuing
-        // many small copies is the slower path). Digitising: lane = 8 o + q, case q, beta / degree
-        // octet o of the chunk (a quarter warp reads the eight cases of one octet: distinct banks).
-        const int L = warp - kLoadWarp0;
-        const int q = lane & 7, o = lane >> 3;
-        auto issue = [&](const Loc& Lc, int sl) {
-            if (Lc.idx < 0) return;
-            const ItemGeo& it = Lc.it;
-            const int c = Lc.c, N = it.N;
-            unsigned char* base = smem + kOffRaw + sl * kRawBytes;
-            uint64_t* bar = &bars[kBarRawFull + sl];
-            const int len = min(kKC, N - kKC * c);   // forward: beta samples of this chunk
-            const uint32_t per_t = DIR == 0 ? (uint32_t)(kRawHdr + it.nc * len * 16) : (uint32_t)kRawT;
-            tc::fence_proxy_async();   // this warp's reads of the slot come before the copies into it
-            if (lane == 0) tc::mbar_arrive_expect_tx(bar, per_t * (uint32_t)it.nt);
-            __syncwarp();
-            if (DIR == 1) {
-                // the chunk block of transform `lane`: header and data in one copy
-                if (lane < it.nt)
-                    tc::bulk_g2s(base + lane * kRawT,
-                                 aux_of(it.gr, it.t0 + lane) + aux_inv(it.B) +
-                                     (size_t)(inv_chunk_prefix(it.B, it.M, it.Mp) + c) * kInvChunk,
-                                 (uint32_t)kRawT, bar);
-            } else {
-                // lane 9 t + j: j < 8 the chunk of case j's bin column, j = 8 the scale header
-                const int t = lane / 9, j = lane - 9 * (lane / 9);
-                if (t < it.nt) {
-                    if (j == 8) {
-                        tc::bulk_g2s(base + t * kRawT, aux_of(it.gr, it.t0 + t) + (size_t)2 * 8 * it.cls, kRawHdr, bar);
-                    } else if (j < it.nc) {
-                        const PairCase p = class_case(it.M, it.Mp, j, N);
-                        const int k0 = p.rev ? N - kKC * c - len : kKC * c;
-                        tc::bulk_g2s(base + t * kRawT + kRawHdr + j * kRawPitch,
-                                     it.gr->X[it.t0 + t] + ((size_t)p.row * N + p.col) * N + k0, (uint32_t)len * 16u, bar);
-                    }
-                }
-            }
-            __syncwarp();
-        };
-        int nis0 = 0, nis1 = 0;   // copies issued into this warp's two slots
-        Loc cur, nxt;
-        locate<DIR>(cur, 0, L, groups, segs, s_first, nseg, n_items, hint);
-        nxt.idx = -1;
-        if (cur.idx >= 0) locate<DIR>(nxt, cur.r, cur.c + kLoadWarps, groups, segs, s_first, nseg, n_items, hint);
-        if (cur.idx >= 0) {
-            issue(cur, kRawPerWarp * L);
-            ++nis0;
-        }
-        if (nxt.idx >= 0) {
-            issue(nxt, kRawPerWarp * L + 1);
-            ++nis1;
-        }
-        int g = L;
-        for (int j = 0; cur.idx >= 0 && !*s_abort; ++j) {
-            const int sl = kRawPerWarp * L + (j & 1);
-            const int s = g % kStages, us = g / kStages;
-            if (!tc::mbar_wait_bounded(&bars[kBarRawFull + sl], (uint32_t)((j >> 1) & 1), kWaitNs, s_abort) ||
-                !tc::mbar_wait_bounded(&bars[kBarEmpty + s], (uint32_t)((us & 1) ^ 1), kWaitNs, s_abort))
-                break;
+    } else if (warp == kLoadWarp) {
+        // ------------------------------------------------------------------ copies (data operand)
+        // Every chunk of the ring in order: once its stage is empty, one bulk copy brings the
+        // chunk's digit block (both transforms of the pair) into the stage's B operand; copy[s]
+        // completes on the byte count.
+        Loc cur;
+        locate<DIR>(cur, 0, 0, groups, segs, s_seg, nseg, n_items, hint);
+        int g = 0;
+        for (; cur.idx >= 0 && !*s_abort; ++g) {
+            const int s = g % kStages, u = g / kStages;
+            if (!tc::mbar_wait_bounded(&bars[kBarEmpty + s], (uint32_t)((u & 1) ^ 1), kWaitNs, s_abort)) break;
             const ItemGeo& it = cur.it;
-            const int N = it.N;
-            const PairCase p = class_case(it.M, it.Mp, q < it.nc ? q : 0, N);
-            const unsigned char* raw = smem + kOffRaw + sl * kRawBytes;
-            unsigned char* Bm = smem + s * kStageBytes + kABytes;
-            const int len = min(kKC, N - kKC * cur.c);
-            for (int t = 0; t < it.nt; ++t) {
-                if (q >= it.nc) continue;   // rows of absent cases are never read back
-                const double2 cs = *reinterpret_cast<const double2*>(raw + t * kRawT + 32 * q);
-                const double2* col = reinterpret_cast<const double2*>(raw + t * kRawT + kRawHdr + q * kRawPitch);
-                double zr[8], zi[8];
-#pragma unroll
-                for (int i = 0; i < 8; ++i) {
-                    const int kk = 8 * o + i;   // position in the chunk
-                    double2 v = make_double2(0.0, 0.0);
-                    if (DIR == 0) {
-                        if (kk < len) v = col[p.rev ? len - 1 - kk : kk];
-                    } else {
-                        v = col[kk];   // zero past the class's last degree
-                    }
-                    zr[i] = fma(v.x, cs.x, kMagic);
-                    zi[i] = fma(v.y, cs.y, kMagic);
-                }
-                const int n = 16 * t + 2 * q;   // re row of plane 0; im is n + 1; plane p at + 16 nt p
-                unsigned char* unit = Bm + (n >> 3) * 256 + (o >> 1) * 128 + (n & 7) * 16 + (o & 1) * 8;
-                store_unit8(unit, 512 * it.nt, zr);
-                store_unit8(unit + 16, 512 * it.nt, zi);
+            if (lane == 0) {
+                const long long j = DIR == 0 ? (long long)it.cls * fwd_chunks(it.N) + cur.c
+                                             : inv_chunk_prefix(it.B, it.M, it.Mp) + cur.c;
+                const unsigned char* src = reinterpret_cast<const unsigned char*>(
+                                               aux_of(it.gr, dig_block_owner(it.t0, it.nt, j)) + aux_dig(it.B)) +
+                                           dig_block_off(it.nt, j);
+                const uint32_t bytes = (uint32_t)(kDigT * it.nt);
+                tc::mbar_arrive_expect_tx(&bars[kBarCopy + s], bytes);
+                tc::bulk_g2s(smem + s * kStageBytes + kABytes, src, bytes, &bars[kBarCopy + s]);
             }
-            tc::fence_proxy_async();
             __syncwarp();
-            if (lane == 0) tc::mbar_arrive(&bars[kBarFull + s]);
-            // chunk j + 2 of this warp into the slot just read
-            Loc n2;
-            n2.idx = -1;
-            if (nxt.idx >= 0) locate<DIR>(n2, nxt.r, nxt.c + kLoadWarps, groups, segs, s_first, nseg, n_items, hint);
-            if (n2.idx >= 0) {
-                issue(n2, sl);
-                if (j & 1)
-                    ++nis1;
-                else
-                    ++nis0;
+            advance<DIR>(cur, 1, groups, segs, s_seg, nseg, n_items, hint);
+        }
+        // the copies of the last phases armed on each stage have landed before the CTA can end
+        if (lane == 0)
+            for (int k = 1; k <= kStages && g - k >= 0; ++k) {
+                const int gg = g - k;
+                const uint64_t t0 = tc::globaltimer_ns();
+                while (!tc::mbar_try_wait(&bars[kBarCopy + gg % kStages], (uint32_t)((gg / kStages) & 1)))
+                    if (tc::globaltimer_ns() - t0 > kWaitNs) break;
             }
-            cur = nxt;
-            nxt = n2;
-            g += kLoadWarps;
-        }
-        // the copies of each slot's last armed phase have landed before the CTA can end
-        for (int k = 0; k < kRawPerWarp; ++k) {
-            const int ni = k == 0 ? nis0 : nis1;
-            if (ni == 0) continue;
-            const uint64_t t0 = tc::globaltimer_ns();
-            while (!tc::mbar_try_wait(&bars[kBarRawFull + kRawPerWarp * L + k], (uint32_t)((ni - 1) & 1)))
-                if (tc::globaltimer_ns() - t0 > kWaitNs) break;
-        }
+        __syncwarp();
     } else if (warp >= kEpiWarp0 && warp < kEpiWarp0 + 4) {
         // ------------------------------------------------------------------ epilogue
         // The next item's column scales (lane i < 16: transform i / 8, case i % 8) and, forward, the
@@ -604,7 +535,7 @@ __global__ void __launch_bounds__(kThreads, 1)
             for (;; ++r) {
                 const int idx = cta_item(r, n_items);
                 if (idx < 0) return -1;
-                if (item_geo<DIR>(groups, segs, s_first, nseg, idx, hint).nchunks > 0) return idx;
+                if (item_geo<DIR>(groups, segs, s_seg, nseg, idx, hint).nchunks > 0) return idx;
             }
         };
         auto load_scales = [&](const ItemGeo& it, double2& ics, double& rowf) {
@@ -621,7 +552,7 @@ __global__ void __launch_bounds__(kThreads, 1)
         double2 ics_c = make_double2(1.0, 1.0);
         double rowf_c = 0.0;
         if (idx >= 0) {
-            it = item_geo<DIR>(groups, segs, s_first, nseg, idx, hint);
+            it = item_geo<DIR>(groups, segs, s_seg, nseg, idx, hint);
             load_scales(it, ics_c, rowf_c);
         }
         int n = 0;
@@ -632,7 +563,7 @@ __global__ void __launch_bounds__(kThreads, 1)
             double2 ics_n = make_double2(1.0, 1.0);
             double rowf_n = 0.0;
             if (nidx >= 0) {
-                nit = item_geo<DIR>(groups, segs, s_first, nseg, nidx, hint);
+                nit = item_geo<DIR>(groups, segs, s_seg, nseg, nidx, hint);
                 load_scales(nit, ics_n, rowf_n);
             }
             const int a = n & 1, ua = n >> 1;
@@ -700,13 +631,14 @@ __global__ void __launch_bounds__(kThreads, 1)
             ics_c = ics_n;
             rowf_c = rowf_n;
         }
-    } else if (warp >= kGenWarp0) {
+    } else if (warp >= kGenWarp0 || (DIR == 0 && warp > kLoadWarp && warp < kEpiWarp0)) {
         // ------------------------------------------------------------------ generators (Wigner rows)
         // The recurrence coefficients and row scales of 32 steps at a time are loaded by the warp's
         // lanes in one coalesced load (a batch ahead, into registers) and published to the warp's
         // shared-memory slot; the steps read them from there, so no step waits on global memory.
         // Rows past the class's last degree get zero coefficients and a zero row scale.
-        const int w = warp - kGenWarp0;
+        constexpr int GW = DIR == 0 ? kGenWarpsFwd : kGenWarpsInv;
+        const int w = warp >= kGenWarp0 ? warp - kGenWarp0 : kGenWarpsInv + warp - (kLoadWarp + 1);
         double* s_cf = reinterpret_cast<double*>(smem + kOffCoef) + w * 128;
         double2 pcf = make_double2(0.0, 0.0);
         double pf1 = 0.0, prs = 0.0;
@@ -729,7 +661,7 @@ __global__ void __launch_bounds__(kThreads, 1)
         };
         // The chunks of this warp, in ring order, with the seed inputs and the first coefficient
         // batch of the next one loaded while the current one is generated.
-        auto locate_g = [&](Loc& L, int r, int c) { locate<DIR>(L, r, c, groups, segs, s_first, nseg, n_items, hint); };
+        auto locate_g = [&](Loc& L, int r, int c) { locate<DIR>(L, r, c, groups, segs, s_seg, nseg, n_items, hint); };
         struct SeedIn {
             double cb, wk, nf;
             double2 ps, pc;
@@ -770,7 +702,12 @@ __global__ void __launch_bounds__(kThreads, 1)
         fetch_loc(cur, 0);
         while (cur.idx >= 0 && !*s_abort) {
             Loc nx;
-            locate_g(nx, DIR == 0 ? cur.r : cur.r + 1, DIR == 0 ? cur.c + kGenWarps : 0);
+            if (DIR == 0) {
+                nx = cur;
+                advance<DIR>(nx, GW, groups, segs, s_seg, nseg, n_items, hint);
+            } else {
+                locate_g(nx, cur.r + 1, 0);
+            }
             SeedIn sn;
             load_seed(nx, sn);
             const ItemGeo& it = cur.it;
@@ -823,7 +760,7 @@ __global__ void __launch_bounds__(kThreads, 1)
                 tc::fence_proxy_async();
                 __syncwarp();
                 if (lane == 0) tc::mbar_arrive(&bars[kBarFull + s]);
-                g += kGenWarps;
+                g += GW;
             } else {
                 // inverse: beta column k of the tile for this lane, 32 degrees per chunk
                 const int m = 32 * w + lane;
@@ -875,62 +812,118 @@ __global__ void __launch_bounds__(kThreads, 1)
     }
 }
 
-// Forward column scales: for every (class, case) the largest |re|, |im| over beta of its bin
-// column, as {scale * 2^47} and {1 / scale} into the transform's scale table. One warp per
-// (class, case), gridDim.z = transforms.
-__global__ void split_fwd_scales_kernel(double2* const* X, int B)
+// Digits of one value pair (re, im of chunk position k = lane, case q) into the shared-memory image
+// of a class's digit blocks for one transform: chunk i at i * 3072, plane p at + 512 p, rows
+// 2q (re) and 2q + 1 (im) in the B operand's layout.
+__device__ __forceinline__ void digits_to_image(unsigned char* img, int i, int q, int lane, double2 v, double2 cs)
 {
-    const int N = 2 * B;
-    const long long wid = (long long)blockIdx.x * 8 + (threadIdx.x >> 5);
-    const int lane = threadIdx.x & 31;
-    if (wid >= (long long)num_classes(B) * 8) return;
-    const int cls = (int)(wid >> 3), q = (int)(wid & 7);
-    int M, Mp;
-    class_orders(cls, M, Mp);
-    double mre = 0.0, mim = 0.0;
-    if (q < class_case_count(M, Mp)) {
-        const PairCase p = class_case(M, Mp, q, N);
-        const double2* col = X[blockIdx.z] + ((size_t)p.row * N + p.col) * N;
-        for (int k = lane; k < N; k += 32) {
-            const double2 v = __ldg(col + k);
-            mre = fmax(mre, fabs(v.x));
-            mim = fmax(mim, fabs(v.y));
-        }
+    const double zr = fma(v.x, cs.x, kMagic), zi = fma(v.y, cs.y, kMagic);
+    const unsigned long long br = (unsigned long long)__double_as_longlong(zr);
+    const unsigned long long bi = (unsigned long long)__double_as_longlong(zi);
+    const int r = 2 * q;
+    unsigned char* u = img + i * kDigT + (r >> 3) * 256 + (lane >> 4) * 128 + (r & 7) * 16 + (lane & 15);
+#pragma unroll
+    for (int p = 0; p < kPlanes; ++p) {   // plane p: byte 5 - p, most significant first
+        u[p * 512] = (unsigned char)(br >> (8 * (5 - p))) ^ 0x80;
+        u[p * 512 + 16] = (unsigned char)(bi >> (8 * (5 - p))) ^ 0x80;
     }
+}
+
+// The image of `nch` chunks (first chunk j0 of the class-major list) to the digit blocks of
+// transform t of a group of T: plane p of chunk i to its block at 512 (nt p + h), 512 bytes per
+// warp store. All threads of the CTA.
+__device__ __forceinline__ void image_to_blocks(const unsigned char* img, double2* const* X, int t, int T, int B,
+                                                long long j0, int nch)
+{
+    const size_t N = (size_t)(2 * B);
+    const int t0 = t & ~1, nt = T - t0 < kNT ? T - t0 : kNT, h = t - t0;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    for (int pc = warp; pc < nch * kPlanes; pc += (int)(blockDim.x >> 5)) {
+        const int i = pc / kPlanes, p = pc - kPlanes * i;
+        const long long j = j0 + i;
+        unsigned char* blk = reinterpret_cast<unsigned char*>(X[dig_block_owner(t0, nt, j)] + N * N * N + aux_dig(B)) +
+                             dig_block_off(nt, j);
+        const uint4 v = reinterpret_cast<const uint4*>(img + i * kDigT + p * 512)[lane];
+        reinterpret_cast<uint4*>(blk + 512 * (nt * p + h))[lane] = v;
+    }
+}
+
+// Column scale entries of (class, case) {scale * 2^47 re, im}, {1 / scale re, im} from the
+// column's largest |re|, |im| (the warp's lanes' maxima reduced here).
+__device__ __forceinline__ double2 column_scales(double mre, double mim, double2* tab_entry, int lane)
+{
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) {
         mre = fmax(mre, __shfl_xor_sync(0xffffffffu, mre, o));
         mim = fmax(mim, __shfl_xor_sync(0xffffffffu, mim, o));
     }
+    double cr, ci, ir, ii;
+    column_scale(mre, cr, ir);
+    column_scale(mim, ci, ii);
     if (lane == 0) {
-        double cr, ci, ir, ii;
-        column_scale(mre, cr, ir);
-        column_scale(mim, ci, ii);
-        double2* tab = X[blockIdx.z] + (size_t)N * N * N + (size_t)2 * wid;
-        tab[0] = make_double2(cr, ci);
-        tab[1] = make_double2(ir, ii);
+        tab_entry[0] = make_double2(cr, ci);
+        tab_entry[1] = make_double2(ir, ii);
     }
+    return make_double2(cr, ci);
+}
+
+// Forward operand: for every class, the bin columns of its eight cases over beta (chunk position k
+// holds beta k, or N - 1 - k for a reversed case; zero past N and for absent cases), their column
+// scales into the scale table and their digits into the class's ceil(N / 32) <= NCM digit blocks.
+// One CTA of eight warps (warp = case) per (class, transform), gridDim.z = the group's T
+// transforms; lane k reads position 32 i + k of its column (coalesced), the digits go through a
+// shared-memory image of the blocks and leave as whole 512-byte plane pieces. Dynamic shared
+// memory NCM * 3072 bytes.
+template <int NCM>
+__global__ void __launch_bounds__(256, NCM == 8 ? 4 : 3) split_fwd_prepare_kernel(double2* const* X, int B, int T)
+{
+    extern __shared__ __align__(16) unsigned char img[];
+    const int N = 2 * B, NC = fwd_chunks(N);
+    const int cls = blockIdx.x, t = blockIdx.z, q = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    int M, Mp;
+    class_orders(cls, M, Mp);
+    const bool live = q < class_case_count(M, Mp);
+    const PairCase p = class_case(M, Mp, live ? q : 0, N);
+    const double2* col = X[t] + ((size_t)p.row * N + p.col) * N;
+    double2 v[NCM];
+    double mre = 0.0, mim = 0.0;
+#pragma unroll
+    for (int i = 0; i < NCM; ++i) {
+        v[i] = make_double2(0.0, 0.0);
+        const int k = kKC * i + lane;
+        if (i < NC && live && k < N) {
+            v[i] = __ldg(col + (p.rev ? N - 1 - k : k));
+            mre = fmax(mre, fabs(v[i].x));
+            mim = fmax(mim, fabs(v[i].y));
+        }
+    }
+    double2* tab = X[t] + (size_t)N * N * N + (size_t)2 * (8 * cls + q);
+    const double2 cs = column_scales(mre, mim, tab, lane);
+#pragma unroll
+    for (int i = 0; i < NCM; ++i)
+        if (i < NC) digits_to_image(img, i, q, lane, v[i], cs);
+    __syncthreads();
+    image_to_blocks(img, X, t, T, B, (long long)cls * NC, NC);
 }
 
 // Inverse operand: for every (class, case) the column G[l] = (2B^2/pi) sign(l) f^l / (row scale of
-// l), l = M..B-1 (src/fn_idsoft.cpp:109), written class-major (chunk c of the class: 8 cases x 32
-// degrees, zero past B - 1 and for absent cases), and its column scales into the scale table.
-// One warp per (class, case), gridDim.z = transforms; the row table must be written first.
-__global__ void split_inv_prepare_kernel(double2* const* X, const double2* const* coeffs, int B)
+// l), l = M..B-1 (src/fn_idsoft.cpp:109; zero past B - 1 and for absent cases), its column scales
+// into the scale table and its digits into the class's ceil((B - M) / 32) digit blocks. One CTA of
+// eight warps (warp = case) per (class, transform), gridDim.z = the group's T transforms; the row
+// table must be written first.
+__global__ void split_inv_prepare_kernel(double2* const* X, const double2* const* coeffs, int B, int T)
 {
+    __shared__ __align__(16) unsigned char img[8 * kDigT];
     const int N = 2 * B;
-    const long long wid = (long long)blockIdx.x * 8 + (threadIdx.x >> 5);
-    const int lane = threadIdx.x & 31;
-    if (wid >= (long long)num_classes(B) * 8) return;
-    const int cls = (int)(wid >> 3), q = (int)(wid & 7);
+    const int cls = blockIdx.x, t = blockIdx.z, q = threadIdx.x >> 5, lane = threadIdx.x & 31;
     int M, Mp;
     class_orders(cls, M, Mp);
     const int nch = (B - M + kKC - 1) / kKC;
-    double2* aux = X[blockIdx.z] + (size_t)N * N * N;
+    double2* aux = X[t] + (size_t)N * N * N;
     const double2* rows = aux + aux_rows(B);
     const bool live = q < class_case_count(M, Mp);
     const PairCase p = class_case(M, Mp, live ? q : 0, N);
-    const double2* cf = coeffs[blockIdx.z];
+    const double2* cf = coeffs[t];
     const double norm = (double)(B * 2 * B) / kPi;
     double2 v[8];
     double mre = 0.0, mim = 0.0;
@@ -946,27 +939,12 @@ __global__ void split_inv_prepare_kernel(double2* const* X, const double2* const
             mim = fmax(mim, fabs(v[i].y));
         }
     }
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-        mre = fmax(mre, __shfl_xor_sync(0xffffffffu, mre, o));
-        mim = fmax(mim, __shfl_xor_sync(0xffffffffu, mim, o));
-    }
-    double2* blk = aux + aux_inv(B) + (size_t)inv_chunk_prefix(B, M, Mp) * kInvChunk;
+    const double2 cs = column_scales(mre, mim, aux + (size_t)2 * (8 * cls + q), lane);
 #pragma unroll
     for (int i = 0; i < 8; ++i)
-        if (i < nch) blk[(size_t)i * kInvChunk + kRawHdr / 16 + q * (kRawPitch / 16) + lane] = v[i];
-    double cr, ci, ir, ii;
-    column_scale(mre, cr, ir);
-    column_scale(mim, ci, ii);
-    // the entry goes to the scale table (epilogue) and into the header of each of the class's chunks
-    if (lane == 0) {
-        aux[2 * wid] = make_double2(cr, ci);
-        aux[2 * wid + 1] = make_double2(ir, ii);
-    }
-    if (lane < 2 * nch) {
-        double2* h = blk + (size_t)(lane >> 1) * kInvChunk + 2 * q + (lane & 1);
-        *h = (lane & 1) ? make_double2(ir, ii) : make_double2(cr, ci);
-    }
+        if (i < nch) digits_to_image(img, i, q, lane, v[i], cs);
+    __syncthreads();
+    image_to_blocks(img, X, t, T, B, inv_chunk_prefix(B, M, Mp), nch);
 }
 
 // Row scales of the generated operand, {0.49 / bound * 2^47, bound / 0.49} per degree l, bound =
@@ -1002,7 +980,7 @@ bool dwt_split_supported(int B) { return B >= 1 && B <= 256; }
 
 size_t dwt_split_aux_elems(int B)
 {
-    return aux_inv(B) + (size_t)kInvChunk * (size_t)inv_chunk_prefix(B, B, 0);
+    return aux_dig(B) + (size_t)(kDigPair / 16) * (size_t)((dig_chunks(B) + 1) / 2);
 }
 
 cudaError_t dwt_split_scales(int direction, int B, int T, double2* const* d_ws, const double2* const* d_coeffs,
@@ -1011,11 +989,14 @@ cudaError_t dwt_split_scales(int direction, int B, int T, double2* const* d_ws, 
     split_rows_kernel<<<dim3(1, 1, (unsigned)T), 256, 0, s>>>(d_ws, w, B, direction == 0 ? 1 : 0);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
-    dim3 grid((unsigned)((num_classes(B) * 8 + 7) / 8), 1, (unsigned)T);
+    dim3 grid((unsigned)num_classes(B), 1, (unsigned)T);
     if (direction == 0)
-        split_fwd_scales_kernel<<<grid, 256, 0, s>>>(d_ws, B);
+        if (fwd_chunks(2 * B) <= 8)
+            split_fwd_prepare_kernel<8><<<grid, 256, (size_t)fwd_chunks(2 * B) * kDigT, s>>>(d_ws, B, T);
+        else
+            split_fwd_prepare_kernel<16><<<grid, 256, (size_t)fwd_chunks(2 * B) * kDigT, s>>>(d_ws, B, T);
     else
-        split_inv_prepare_kernel<<<grid, 256, 0, s>>>(d_ws, d_coeffs, B);
+        split_inv_prepare_kernel<<<grid, 256, 0, s>>>(d_ws, d_coeffs, B, T);
     return cudaGetLastError();
 }
 
