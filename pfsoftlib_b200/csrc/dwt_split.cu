@@ -130,6 +130,9 @@ constexpr double kTwo47 = 140737488355328.0;        // 2^47
 // 2^52 + sum_{i<6} 128 * 256^i: adding it to x * 2^47 (|x| < 0.5) leaves round(x * 2^47) + C in
 // the low 48 bits of the double, C making every byte a digit plus 128.
 constexpr double kMagic = 4503599627370496.0 + 141289400074368.0;
+// An integer x with |x| < 2^51 added to the bit pattern of 2^52 + 2^51 is that double plus x.
+constexpr long long kI2DBits = 0x4338000000000000LL;
+constexpr double kI2DMagic = 6755399441055744.0;   // 2^52 + 2^51
 
 // One bandwidth group of a launch: items first .. first+count-1, `pairs` transform pairs (T
 // transforms) and `tiles` tiles per class, bandwidth B, N = 2B.
@@ -369,8 +372,9 @@ __device__ __forceinline__ void gen16(double (&z)[16], double& dcur, double& dpr
 #pragma unroll
     for (int j = 0; j < 16; ++j) {
         const int q = q0 + j;
-        z[j] = fma(sc ? 0.0 : dcur, s_cf[4 * q + 3], kMagic);
-        rec_step(dcur, dprev, cb, *reinterpret_cast<const double2*>(s_cf + 4 * q), s_cf[4 * q + 2]);
+        const double2 fr = *reinterpret_cast<const double2*>(s_cf + 4 * q + 2);   // {f1, row scale}
+        z[j] = fma(sc ? 0.0 : dcur, fr.y, kMagic);
+        rec_step(dcur, dprev, cb, *reinterpret_cast<const double2*>(s_cf + 4 * q), fr.x);
     }
 }
 
@@ -571,7 +575,7 @@ __global__ void __launch_bounds__(kThreads, 1)
             if (!tc::mbar_wait_bounded(&bars[kBarAccFull + a], (uint32_t)(ua & 1), kWaitNs, s_abort)) break;
             tc::fence_after_sync();
             __syncwarp();
-            if (lane < 16) s_ics[lane] = ics_c;
+            if (lane < 16) s_ics[lane] = make_double2(ics_c.x * 0x1p-30, ics_c.y * 0x1p-30);   // powers of two: exact
             const int N = it.N, B = it.B;
             if (lane < it.nc) {   // the item's cases, once per item instead of per lane and value
                 const PairCase p = class_case(it.M, it.Mp, lane, N);
@@ -602,10 +606,14 @@ __global__ void __launch_bounds__(kThreads, 1)
                 double v[16];
 #pragma unroll
                 for (int j = 0; j < 16; ++j) {
-                    // sum_e acc[e] 2^(-8e) = 2^-16 (hi + 2^-24 lo), hi and lo exact in 64 bits
+                    // sum_e acc[e] 2^(-8e) = 2^-16 (hi + 2^-24 lo), hi and lo exact in 64 bits (|.| < 2^43);
+                    // each converted exactly by adding it to the bits of 2^52 + 2^51 (FP64 add, no
+                    // 64-bit integer conversion); the 2^-30 (2^-16 and the digits' 2^-14) rides in ics
                     const long long hi = (long long)acc[0][j] * 65536 + (long long)acc[1][j] * 256 + acc[2][j];
                     const long long lo = (long long)acc[3][j] * 65536 + (long long)acc[4][j] * 256 + acc[5][j];
-                    v[j] = fma((double)lo, 0x1p-24, (double)hi) * 0x1p-30;   // and the digits' 2^-14
+                    const double hd = __longlong_as_double(hi + kI2DBits) - kI2DMagic;
+                    const double ld = __longlong_as_double(lo + kI2DBits) - kI2DMagic;
+                    v[j] = fma(ld, 0x1p-24, hd);
                 }
                 if (!live) continue;
 #pragma unroll
