@@ -971,9 +971,11 @@ def main():
     gout = torch.empty_like(gh).pin_memory()
     fout = torch.empty_like(fh).pin_memory()
     errs = []
+    start = threading.Barrier(2)
 
     def worker(fn):
         try:
+            start.wait()   # both threads leave together: no thread-start skew inside the timed span
             for _ in range(e2e_steps):
                 if fn():
                     raise RuntimeError(lib.pfsoft_last_error().decode())

@@ -366,17 +366,19 @@ __global__ void __launch_bounds__(kWarps * 32, inv_min_blocks(KT, TW, CS))
                 bv1[n] = gb[4 * GS + v];
             }
             auto mma_step = [&](int s) {
-                // subtiles spread over the 8 steps; the two k-halves of an accumulator are issued
-                // a full round apart so that dependent MMAs do not follow each other
+                // subtiles spread over the 8 steps: step s issues the first k-half of subtile s and
+                // the second k-half of subtile (s + 4) mod 8, so that the two MMAs into one
+                // accumulator are four steps apart (measured: -2 % per B=128 iDSOFT against both
+                // halves in the same step); subtiles with p % 8 >= 4 thus take their second half
+                // first, as dwt_batch_kernel does too
                 constexpr int PS = (NSUB8 + 7) / 8;
+                const int s1 = (s + 4) & 7;
                 double av0[PS], av1[PS];
 #pragma unroll
                 for (int i = 0; i < PS; ++i) {
-                    const int p = s + 8 * i;
-                    if (p < NSUB8) {
-                        av0[i] = dc[t4 * DS + 8 * p + g];
-                        av1[i] = dc[(4 + t4) * DS + 8 * p + g];
-                    }
+                    const int p = s + 8 * i, p1 = s1 + 8 * i;
+                    if (p < NSUB8) av0[i] = dc[t4 * DS + 8 * p + g];
+                    if (p1 < NSUB8) av1[i] = dc[(4 + t4) * DS + 8 * p1 + g];
                 }
 #pragma unroll
                 for (int i = 0; i < PS; ++i) {
@@ -388,10 +390,10 @@ __global__ void __launch_bounds__(kWarps * 32, inv_min_blocks(KT, TW, CS))
                 }
 #pragma unroll
                 for (int i = 0; i < PS; ++i) {
-                    const int p = s + 8 * i;
-                    if (p < NSUB8) {
+                    const int p1 = s1 + 8 * i;
+                    if (p1 < NSUB8) {
 #pragma unroll
-                        for (int n = 0; n < NT; ++n) dmma(acc[p][n][0], acc[p][n][1], av1[i], bv1[n]);
+                        for (int n = 0; n < NT; ++n) dmma(acc[p1][n][0], acc[p1][n][1], av1[i], bv1[n]);
                     }
                 }
             };

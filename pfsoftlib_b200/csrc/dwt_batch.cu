@@ -246,13 +246,15 @@ __global__ void __launch_bounds__(64 * TT) dwt_batch_kernel(const DwtGroup* __re
                         const double* d0 = s_d + (b0 + t4) * DS + g;
                         const double* d1 = s_d + (b0 + 4 + t4) * DS + g;
                         // narrower bandwidths in a wider launch skip empty tiles; the two k-halves
-                        // of an accumulator are issued a full round apart
+                        // of an accumulator are issued a full round apart, the second half first
+                        // for subtiles with p % 8 >= 4: the order dwt_inverse_kernel sums them in,
+                        // so that a transform gives the same bits batched or alone
 #pragma unroll
                         for (int p = 0; p < NSUB8; ++p)
-                            if (8 * p < N) dmma(acc[p][0], acc[p][1], d0[8 * p], bv0);
+                            if (8 * p < N) dmma(acc[p][0], acc[p][1], (p & 4) ? d1[8 * p] : d0[8 * p], (p & 4) ? bv1 : bv0);
 #pragma unroll
                         for (int p = 0; p < NSUB8; ++p)
-                            if (8 * p < N) dmma(acc[p][0], acc[p][1], d1[8 * p], bv1);
+                            if (8 * p < N) dmma(acc[p][0], acc[p][1], (p & 4) ? d0[8 * p] : d1[8 * p], (p & 4) ? bv0 : bv1);
                     }
                 }
                 __syncthreads();   // tile and coefficient chunk are rewritten by the next chunk
