@@ -473,11 +473,8 @@ int run_idsoft(const double* d_coeffs, int B, double* d_grid, void* ws, cudaStre
     const long long n = N, n2 = n * n;
     double2* X = static_cast<double2*>(ws);
     double2* G = reinterpret_cast<double2*>(d_grid);
-    {
-        StageScope sc(ST_NYQUIST, s);
-        PF_CUDA(zero_nyquist_launch(X, B, s));
-    }
     DwtArgs a = dwt_args(t);
+    a.zero_nyquist = 1;   // the Nyquist bins, which no order class writes, zeroed in the DWT's tail
     {
         StageScope sc(ST_DWT_INV, s);
         PF_CUDA(dwt_inverse_launch(reinterpret_cast<const double2*>(d_coeffs), X, a, 0, s));

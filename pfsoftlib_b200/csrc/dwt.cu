@@ -257,6 +257,28 @@ __global__ void __launch_bounds__(kWarps * 32, fwd_min_blocks(KT, TW, CS))
     }
 }
 
+// The Nyquist bins of X (row B with every column, column B with every other row; every beta),
+// which no order class writes: set to zero, element i = first, first + stride, ...
+__device__ __forceinline__ void nyquist_zero(double2* X, int B, long long first, long long stride)
+{
+    const int N = 2 * B;
+    const long long total = (long long)(2 * N - 1) * N;
+    for (long long i = first; i < total; i += stride) {
+        const long long v = i / N;
+        const int k = (int)(i - v * N);
+        int row, col;
+        if (v < N) {
+            row = B;
+            col = (int)v;
+        } else {
+            col = B;
+            row = (int)(v - N);
+            if (row >= B) ++row;   // skip (B, B), covered above
+        }
+        X[((size_t)row * N + col) * N + k] = make_double2(0.0, 0.0);
+    }
+}
+
 // Inverse DWT (see the header comment). Each lane ends with case 4n + t4 of its n-tiles at
 // columns cw*KW + 8p + g. The rows of 8-degree block b+1 are generated while block b is
 // applied (two MMA k-steps of 4 degrees). Coefficients move through registers one 32-degree
@@ -441,26 +463,12 @@ __global__ void __launch_bounds__(kWarps * 32, inv_min_blocks(KT, TW, CS))
         M = M2;
         Mp = Mp2;
     }
+    if (a.zero_nyquist) nyquist_zero(X, B, (long long)blockIdx.x * blockDim.x + threadIdx.x, (long long)gridDim.x * blockDim.x);
 }
 
 __global__ void zero_nyquist_kernel(double2* X, int B)
 {
-    const int N = 2 * B;
-    const long long total = (long long)(2 * N - 1) * N;
-    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total; i += (long long)gridDim.x * blockDim.x) {
-        const long long v = i / N;
-        const int k = (int)(i - v * N);
-        int row, col;
-        if (v < N) {
-            row = B;
-            col = (int)v;
-        } else {
-            col = B;
-            row = (int)(v - N);
-            if (row >= B) ++row;   // skip (B, B), covered above
-        }
-        X[((size_t)row * N + col) * N + k] = make_double2(0.0, 0.0);
-    }
+    nyquist_zero(X, B, blockIdx.x * (long long)blockDim.x + threadIdx.x, (long long)gridDim.x * blockDim.x);
 }
 
 // Resident CTAs on all SMs (the persistent grid).
@@ -517,6 +525,7 @@ DwtArgs dwt_args_for(const BandTables& t)
     a.rc_f1 = t.rc_f1;
     a.classes = nullptr;
     a.n_classes = 0;
+    a.zero_nyquist = 0;
     return a;
 }
 

@@ -56,6 +56,9 @@ struct DwtArgs {
     // classes[0 .. n_classes-1] only and leave every other class's outputs untouched.
     const int* classes;
     int n_classes;
+    // Inverse only: also zero the Nyquist bins (row B or column B of X, which no order class
+    // writes) in the kernel's tail, instead of a separate launch.
+    int zero_nyquist;
 };
 
 // Arguments of the DWT launches over every order class of a bandwidth's tables.
