@@ -29,6 +29,9 @@ struct FftPassArgs {
     const double2* const* srcs;
     double2* const* dsts;
     int coherent;                // first-stage loads through the coherent path (0: read-only path)
+    // last-stage stores marked evict-first (st.global.cs): set by fft_pass_launch, whose output is
+    // not read again before it has left L2; left 0 where another pass reads it through L2
+    int stream_out;
     // lengths with a prime factor above 16 (fft_needs_bluestein): Bluestein's chirp tables
     // (fft_bluestein_fill); null keeps the direct O(R^2) stages for that factor
     const double2* bluestein;
