@@ -266,7 +266,7 @@ __global__ void __launch_bounds__(64 * TT) dwt_batch_kernel(const DwtGroup* __re
 #pragma unroll
                 for (int p = 0; p < NSUB8; ++p) {
                     const int k = 8 * p + g;
-                    if (k < N) col[pcase.rev ? N - 1 - k : k] = make_double2(acc[p][0], acc[p][1]);
+                    if (k < N) __stcs(col + (pcase.rev ? N - 1 - k : k), make_double2(acc[p][0], acc[p][1]));   // evict-first, as dwt_inverse_kernel
                 }
             }
         }
